@@ -1,0 +1,124 @@
+// Shared device helpers for the GraphGP B200 kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/graphgp_b200.h"
+
+namespace ggp {
+
+constexpr int kWarp = 32;
+
+template <typename T>
+__host__ __device__ __forceinline__ T ceil_div(T a, T b) { return (a + b - 1) / b; }
+
+// ------------------------------------------------------------------------------------------------
+// Device status word. Lives at the start of every workspace; device code reports failures that the
+// host can only see after the stream has run (bounded waits that gave up, NaN outputs).
+// ------------------------------------------------------------------------------------------------
+struct DeviceStatus {
+  unsigned int error;          // a GGP_* status code, 0 = ok
+  unsigned int nan_seen;       // any NaN produced in an output
+  unsigned int fallback_count; // points re-conditioned in FP64 (pivot below threshold)
+  unsigned int timeouts;       // bounded waits that ran out
+  unsigned int ticket;         // work counter for persistent kernels
+  unsigned int ticket2;
+  unsigned int pad[58];        // keeps the struct at 256 bytes
+};
+static_assert(sizeof(DeviceStatus) == 256, "status block must be 256 bytes");
+
+// ------------------------------------------------------------------------------------------------
+// "Not yet computed" markers. A value slot holds this quiet-NaN payload until its producer stores
+// the real value; arithmetic on the device only yields the canonical NaN (0x7fffffff / 0x7ff8...),
+// and every producer canonicalises NaN, so a stored value never equals the marker.
+// ------------------------------------------------------------------------------------------------
+constexpr uint32_t kPendingF32 = 0x7fa5c3e1u;
+constexpr uint64_t kPendingF64 = 0x7ff4a5c3e1d2b6f7ull;
+
+__device__ __forceinline__ float pending_value(float) { return __uint_as_float(kPendingF32); }
+__device__ __forceinline__ double pending_value(double) { return __longlong_as_double((long long)kPendingF64); }
+__device__ __forceinline__ bool is_pending(float v) { return __float_as_uint(v) == kPendingF32; }
+__device__ __forceinline__ bool is_pending(double v) { return (uint64_t)__double_as_longlong(v) == kPendingF64; }
+
+__device__ __forceinline__ float canonical(float v) { return (v != v) ? __uint_as_float(0x7fffffffu) : v; }
+__device__ __forceinline__ double canonical(double v) {
+  return (v != v) ? __longlong_as_double(0x7ff8000000000000ll) : v;
+}
+
+// Relaxed, L1-bypassing load / store at GPU scope: the value itself is the ready flag.
+__device__ __forceinline__ float ld_relaxed(const float* p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ double ld_relaxed(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(float* p, float v) {
+  asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(int* p, int v) {
+  asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait until a value slot is no longer pending. Returns false if the wait ran out; the caller
+// then records GGP_ERR_TIMEOUT and produces NaN so that nothing downstream waits on it.
+template <typename T>
+__device__ __forceinline__ bool wait_ready(const T* slot, T& out, uint64_t timeout_ns) {
+  T v = ld_relaxed(slot);
+  if (!is_pending(v)) { out = v; return true; }
+  const uint64_t t0 = global_timer_ns();
+  unsigned int backoff = 32;
+  for (unsigned int it = 0; it < (1u << 30); ++it) {
+    __nanosleep(backoff);
+    if (backoff < 512) backoff <<= 1;
+    v = ld_relaxed(slot);
+    if (!is_pending(v)) { out = v; return true; }
+    if (global_timer_ns() - t0 > timeout_ns) break;
+  }
+  out = canonical(v + (T)NAN);
+  return false;
+}
+
+__device__ __forceinline__ void report_error(DeviceStatus* st, unsigned int code) {
+  if (st) atomicCAS(&st->error, 0u, code);
+}
+
+// Warp-level ticket: lane 0 takes the next work item, all lanes get it.
+__device__ __forceinline__ unsigned int warp_ticket(unsigned int* counter) {
+  unsigned int t = 0;
+  if ((threadIdx.x & 31) == 0) t = atomicAdd(counter, 1u);
+  return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// Occupancy-safe persistent grid size for a kernel.
+template <typename Kernel>
+inline int persistent_grid(Kernel k, int block, size_t smem, int max_blocks) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  long g = (long)sms * per_sm;
+  if (max_blocks > 0 && g > max_blocks) g = max_blocks;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+}  // namespace ggp

@@ -1,0 +1,9 @@
+// Explicit instantiations of the register-resident refinement kernels (one unit per shape group,
+// so that the build compiles them in parallel).
+#define GGP_DEFINE_LAUNCHERS
+#include "../refine_launch.cuh"
+
+namespace ggp {
+GGP_INSTANTIATE_FAST(float, 20, 2, false)
+GGP_INSTANTIATE_FAST(float, 20, 3, false)
+}  // namespace ggp

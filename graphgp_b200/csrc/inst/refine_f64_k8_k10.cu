@@ -1,0 +1,11 @@
+// Explicit instantiations of the register-resident refinement kernels (one unit per shape group,
+// so that the build compiles them in parallel).
+#define GGP_DEFINE_LAUNCHERS
+#include "../refine_launch.cuh"
+
+namespace ggp {
+GGP_INSTANTIATE_FAST(double, 8, 2, false)
+GGP_INSTANTIATE_FAST(double, 8, 3, false)
+GGP_INSTANTIATE_FAST(double, 10, 2, false)
+GGP_INSTANTIATE_FAST(double, 10, 3, false)
+}  // namespace ggp

@@ -1,0 +1,528 @@
+// Host launchers and C-ABI entry points for refinement, the dense root and whole-graph generate /
+// inverse / logdet.
+#include <cstdio>
+#include <mutex>
+
+#include "dense.cuh"
+#include "refine_generic.cuh"
+#include "workspace.cuh"
+#include "refine_launch.cuh"
+
+namespace ggp {
+
+// ------------------------------------------------------------------------------------------------
+// small helper kernels
+// ------------------------------------------------------------------------------------------------
+
+// chunk_prefix[b] = chunks (32 rows each) in batches before b; validates the offsets array.
+__global__ void chunk_prefix_kernel(const int* __restrict__ offsets, int n_offsets, long long n0, long long n,
+                                    int* __restrict__ prefix, DeviceStatus* st) {
+  __shared__ long long s_sum[1024];
+  const int nbatch = n_offsets - 1;
+  const int per = (nbatch + blockDim.x - 1) / blockDim.x;
+  const int b0 = threadIdx.x * per;
+  const int b1 = min(nbatch, b0 + per);
+  long long local = 0;
+  bool bad = false;
+  for (int b = b0; b < b1; ++b) {
+    const long long a = offsets[b], c = offsets[b + 1];
+    if (c < a) bad = true;
+    local += (c > a) ? (c - a + 31) / 32 : 0;
+  }
+  s_sum[threadIdx.x] = local;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+    long long v = (threadIdx.x >= (unsigned)o) ? s_sum[threadIdx.x - o] : 0;
+    __syncthreads();
+    s_sum[threadIdx.x] += v;
+    __syncthreads();
+  }
+  long long run = s_sum[threadIdx.x] - local;
+  for (int b = b0; b < b1; ++b) {
+    prefix[b] = (int)run;
+    const long long a = offsets[b], c = offsets[b + 1];
+    run += (c > a) ? (c - a + 31) / 32 : 0;
+  }
+  if (threadIdx.x == blockDim.x - 1) prefix[nbatch] = (int)s_sum[threadIdx.x];
+  if (threadIdx.x == 0) {
+    if (offsets[0] != n0 || offsets[nbatch] > n || offsets[nbatch] < offsets[0]) bad = true;
+  }
+  if (bad) report_error(st, GGP_ERR_INVALID);
+}
+
+template <typename T>
+__global__ void init_values_kernel(T* __restrict__ values, const T* __restrict__ init, long long n0, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    values[i] = (i < n0) ? canonical(init[i]) : pending_value(T(0));
+}
+
+template <typename T>
+__global__ void pending_fill_kernel(T* __restrict__ values, long long from, long long n) {
+  for (long long i = from + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    values[i] = pending_value(T(0));
+}
+
+template <typename T>
+__global__ void gather_kernel(const T* __restrict__ src, const int* __restrict__ perm, T* __restrict__ dst, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[perm ? perm[i] : i];
+}
+
+template <typename T>
+__global__ void copy_kernel(const T* __restrict__ src, T* __restrict__ dst, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+// NaN poisoning (reference refine.py:55, 182): if any output was NaN, every output becomes NaN.
+template <typename T>
+__global__ void poison_kernel(T* __restrict__ out, long long n, const DeviceStatus* st) {
+  if (!st->nan_seen) return;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = canonical((T)NAN);
+}
+
+__global__ void sum_partials_kernel(const double* __restrict__ part, int n, const double* __restrict__ add,
+                                    double* __restrict__ out) {
+  __shared__ double s[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
+    *out = t + (add ? *add : 0.0);
+  }
+}
+
+inline int grid_for(long long n, int block = 256) {
+  long long g = (n + block - 1) / block;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// ------------------------------------------------------------------------------------------------
+// kernel dispatch on (k, d); the register-resident instantiations live in inst_*.cu
+// ------------------------------------------------------------------------------------------------
+template <typename T, int D>
+cudaError_t dispatch_k(const RefineParams<T>& p, int kind, int nb, int max_blocks, cudaStream_t s) {
+  const int k = p.k;
+  switch (k) {
+    case 8: return launch_fast<T, 8, D, false>(p, kind, nb, max_blocks, s);
+    case 10: return launch_fast<T, 10, D, false>(p, kind, nb, max_blocks, s);
+    case 16: return launch_fast<T, 16, D, false>(p, kind, nb, max_blocks, s);
+    case 20: return launch_fast<T, 20, D, false>(p, kind, nb, max_blocks, s);
+    default: break;
+  }
+  if constexpr (sizeof(T) == 4) {
+    if (k == 32) return launch_fast<T, 32, D, false>(p, kind, nb, max_blocks, s);
+    if (k < 16) return launch_fast<T, 16, D, true>(p, kind, nb, max_blocks, s);
+    if (k < 32) return launch_fast<T, 32, D, true>(p, kind, nb, max_blocks, s);
+  } else {
+    if (k < 16) return launch_fast<T, 16, D, true>(p, kind, nb, max_blocks, s);
+  }
+  return launch_generic<T>(p, kind, max_blocks, s);
+}
+
+template <typename T>
+cudaError_t dispatch(const RefineParams<T>& p, int kind, int nb, int max_blocks, cudaStream_t s) {
+  if (p.d == 2) return dispatch_k<T, 2>(p, kind, nb, max_blocks, s);
+  if (p.d == 3) return dispatch_k<T, 3>(p, kind, nb, max_blocks, s);
+  return launch_generic<T>(p, kind, max_blocks, s);
+}
+
+// ------------------------------------------------------------------------------------------------
+// common argument checks
+// ------------------------------------------------------------------------------------------------
+inline int check_refine_args(const void* points, long long n, int d, const void* nbrs, int k, const void* offsets,
+                             int n_offsets, const void* bins, const void* vals, int nb) {
+  if (!points || !bins || !vals) return GGP_ERR_INVALID;
+  if (n < 1 || d < 1 || k < 1 || nb < 2 || n_offsets < 1) return GGP_ERR_INVALID;
+  if (n_offsets > 1 && (!nbrs || !offsets)) return GGP_ERR_INVALID;
+  if (nb > kMaxBins) return GGP_ERR_UNSUPPORTED;
+  if (n > 0x7fffffffLL) return GGP_ERR_UNSUPPORTED;
+  if (generic_smem_bytes(k, d) > 227 * 1024 && !(d == 2 || d == 3)) return GGP_ERR_UNSUPPORTED;
+  if (k > 32 && generic_smem_bytes(k, d) > 227 * 1024) return GGP_ERR_UNSUPPORTED;
+  return GGP_OK;
+}
+
+inline int cuda_status(cudaError_t e) {
+  if (e != cudaSuccess) {
+    fprintf(stderr, "graphgp_b200: CUDA error %s\n", cudaGetErrorString(e));
+    return GGP_ERR_CUDA;
+  }
+  return GGP_OK;
+}
+
+template <typename TB>
+cudaError_t prepare_table(const TB* bins, const TB* vals, int nb, const TableBuffers& tb, cudaStream_t s) {
+  prepare_table_kernel<TB><<<1, 256, 0, s>>>(bins, vals, nb, tb);
+  return cudaGetLastError();
+}
+
+// Refinement core shared by refine / refine_inv / refine_logdet / generate*: expects the status block
+// cleared and the table prepared in `ws`.
+template <typename T>
+RefineParams<T> make_params(const Workspace& ws, const T* points, long long n, int d, const int* nbrs, int k,
+                            const int* offsets, int n_offsets, long long n0, double tau, unsigned long long timeout_ns) {
+  RefineParams<T> p{};
+  p.points = points;
+  p.n = n;
+  p.d = d;
+  p.nbrs = nbrs;
+  p.k = k;
+  p.n0 = n0;
+  p.offsets = offsets;
+  p.n_batches = n_offsets - 1;
+  p.chunk_prefix = ws.chunk_prefix;
+  p.tb = ws.table;
+  p.status = ws.status;
+  p.tau = tau;
+  p.timeout_ns = timeout_ns ? timeout_ns : 10000000000ull;
+  p.logdet_partials = ws.partials;
+  return p;
+}
+
+template <typename T>
+int run_cond(RefineParams<T> p, int mode, int nb, cudaStream_t s) {
+  p.mode = mode;
+  if (p.n_batches < 1 || p.n == p.n0) return GGP_OK;
+  return cuda_status(dispatch<T>(p, kCond, nb, 0, s));
+}
+
+template <typename T>
+int run_logdet(RefineParams<T> p, int nb, double* out, const double* add, cudaStream_t s) {
+  cudaMemsetAsync(p.logdet_partials, 0, sizeof(double) * kMaxPartials, s);
+  if (p.n > p.n0) {
+    cudaError_t e = dispatch<T>(p, kLogdet, nb, kMaxPartials, s);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  sum_partials_kernel<<<1, 1024, 0, s>>>(p.logdet_partials, kMaxPartials, add, out);
+  return cuda_status(cudaGetLastError());
+}
+
+// status reset + table preparation + offsets prefix: the prologue of every refinement-family call
+template <typename T>
+int prologue(const Workspace& ws, const T* bins, const T* vals, int nb, const int* offsets, int n_offsets,
+             long long n0, long long n, cudaStream_t s) {
+  cudaMemsetAsync(ws.status, 0, sizeof(DeviceStatus), s);
+  prepare_table_kernel<T><<<1, 256, 0, s>>>(bins, vals, nb, ws.table);
+  if (n_offsets >= 1 && offsets) chunk_prefix_kernel<<<1, 1024, 0, s>>>(offsets, n_offsets, n0, n, ws.chunk_prefix, ws.status);
+  return cuda_status(cudaGetLastError());
+}
+
+// values[0:n0) = init (canonical), rows [n0, offsets[last]) pending, rows past the last offset 0
+// (the reference's fast_jit path starts from zeros, refine.py:126).
+template <typename T>
+__global__ void init_refine_values_kernel(T* __restrict__ values, const T* __restrict__ init, long long n0, long long n,
+                                          const int* __restrict__ offsets, int n_offsets) {
+  long long last = (n_offsets >= 1 && offsets) ? (long long)offsets[n_offsets - 1] : n0;
+  if (last > n) last = n;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T v;
+    if (i < n0) v = init ? canonical(init[i]) : values[i];
+    else if (i < last) v = pending_value(T(0));
+    else v = T(0);
+    values[i] = v;
+  }
+}
+
+// Dense root on points[0:n0) (graph order). mode 0: out = L xi; 1: out = L^-1 v; 2: logdet.
+template <typename T>
+int dense_root(const Workspace& ws, const T* points, long long n0, int d, int mode, const T* in, const int* perm,
+               T* out_graph, T* out_user, double* out_logdet, cudaStream_t s) {
+  if (n0 <= 0) {
+    if (mode == 2) { cudaMemsetAsync(out_logdet, 0, sizeof(double), s); }
+    return cuda_status(cudaGetLastError());
+  }
+  dense_cov_kernel<T><<<grid_for(n0 * n0), 256, 0, s>>>(points, n0, d, nullptr, ws.table, ws.dense);
+  cudaError_t e = dense_cholesky(ws.dense, n0, s);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (mode == 0) {
+    dense_matvec_kernel<T><<<grid_for(n0 * 32), 256, 0, s>>>(ws.dense, n0, in, perm, out_graph, out_user, ws.status);
+  } else if (mode == 1) {
+    dense_trsv_kernel<T><<<1, 1024, 0, s>>>(ws.dense, n0, in, perm, ws.dense_x, out_graph, out_user, ws.status);
+  } else {
+    dense_logdet_kernel<<<1, 1024, 0, s>>>(ws.dense, n0, out_logdet);
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace ggp
+
+using namespace ggp;
+
+// ------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+int refine_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k, const int32_t* offsets,
+                int n_offsets, const T* bins, const T* vals, int nb, const T* init, const T* xi, T* out, double tau,
+                uint64_t timeout_ns, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !out || !init || (n > n0 && !xi)) return GGP_ERR_INVALID;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_REFINE, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(out, init, n0, n, offsets, n_offsets);
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, timeout_ns);
+  p.values = out;
+  p.xi = xi;
+  return run_cond<T>(p, kGenerate, nb, s);
+}
+
+template <typename T>
+int refine_inv_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k, const int32_t* offsets,
+                    int n_offsets, const T* bins, const T* vals, int nb, const T* values, T* out_init, T* out_xi,
+                    double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !values || !out_init || (n > n0 && !out_xi)) return GGP_ERR_INVALID;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_REFINE_INV, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  if (n0 > 0) copy_kernel<T><<<grid_for(n0), 256, 0, s>>>(values, out_init, n0);
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
+  p.values = const_cast<T*>(values);
+  p.xi_out = out_xi;
+  return run_cond<T>(p, kInverse, nb, s);
+}
+
+template <typename T>
+int refine_logdet_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
+                       const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, double* out,
+                       double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !out) return GGP_ERR_INVALID;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
+  return run_logdet<T>(p, nb, out, nullptr, s);
+}
+
+template <typename T>
+int dense_impl(int mode, const T* points, int64_t n0, int d, const T* bins, const T* vals, int nb, const T* in, T* out,
+               double* out_logdet, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  if (!points || !bins || !vals || n0 < 1 || d < 1 || nb < 2) return GGP_ERR_INVALID;
+  if (nb > kMaxBins) return GGP_ERR_UNSUPPORTED;
+  if (mode < 0 || mode > 2 || (mode < 2 && (!in || !out)) || (mode == 2 && !out_logdet)) return GGP_ERR_INVALID;
+  Workspace ws;
+  int rc = carve_workspace(GGP_OP_DENSE, n0, d, n0, 1, nb, 1, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  cudaMemsetAsync(ws.status, 0, sizeof(DeviceStatus), s);
+  prepare_table_kernel<T><<<1, 256, 0, s>>>(bins, vals, nb, ws.table);
+  return dense_root<T>(ws, points, n0, d, mode, in, nullptr, out, nullptr, out_logdet, s);
+}
+
+template <typename T>
+int generate_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
+                  const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* xi, T* out,
+                  double tau, uint64_t timeout_ns, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !xi || !out) return GGP_ERR_INVALID;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_GENERATE, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  T* vg = (T*)ws.values_graph;
+  // rows >= n0 pending (rows past the last offset 0); rows < n0 come from the dense root below
+  init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, nullptr, n0, n, offsets, n_offsets);
+  if ((rc = dense_root<T>(ws, points, n0, d, 0, xi, perm, vg, out, nullptr, s))) return rc;
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, timeout_ns);
+  p.values = vg;
+  p.xi = xi;
+  p.perm = perm;
+  p.out_user = out;
+  if (!perm) {  // no permutation: xi / out are in graph order already
+    p.perm = nullptr;
+    p.out_user = nullptr;
+    p.xi = xi + n0;
+  }
+  if ((rc = run_cond<T>(p, kGenerate, nb, s))) return rc;
+  if (!perm) copy_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, out, n);
+  poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out, n, ws.status);
+  return cuda_status(cudaGetLastError());
+}
+
+template <typename T>
+int generate_inv_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
+                      const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* values,
+                      T* out_xi, double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !values || !out_xi) return GGP_ERR_INVALID;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_GENERATE_INV, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  T* vg = (T*)ws.values_graph;
+  gather_kernel<T><<<grid_for(n), 256, 0, s>>>(values, perm, vg, n);  // values in graph order
+  // dense part: xi[:n0] = L^-1 v[:n0] (refine.py:186-195), gathered from / scattered to user order
+  if ((rc = dense_root<T>(ws, points, n0, d, 1, values, perm, nullptr, out_xi, nullptr, s))) return rc;
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
+  p.values = vg;
+  p.perm = perm;
+  p.out_user = perm ? out_xi : nullptr;
+  p.xi_out = perm ? nullptr : out_xi + n0;
+  if ((rc = run_cond<T>(p, kInverse, nb, s))) return rc;
+  poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out_xi, n, ws.status);
+  return cuda_status(cudaGetLastError());
+}
+
+template <typename T>
+int generate_logdet_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
+                         const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, double* out,
+                         double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !out) return GGP_ERR_INVALID;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_GENERATE_LOGDET, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  // dense logdet (refine.py:243-248) lands in dense_x[0]; the refined sum adds it (refine.py:238-240)
+  if ((rc = dense_root<T>(ws, points, n0, d, 2, nullptr, nullptr, nullptr, nullptr, ws.dense_x, s))) return rc;
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
+  return run_logdet<T>(p, nb, out, ws.dense_x, s);
+}
+
+}  // namespace
+
+#define GGP_STREAM(s) reinterpret_cast<cudaStream_t>(s)
+
+extern "C" {
+
+const char* ggp_version(void) { return "graphgp_b200 0.1.0 sm_100a"; }
+
+size_t ggp_workspace_size(int op, int64_t n, int d, int64_t n0, int k, int n_bins, int n_offsets, int dtype_bytes) {
+  Workspace ws;
+  if (n_bins < 2) n_bins = 2;
+  if (n_offsets < 1) n_offsets = 1;
+  if (dtype_bytes != 8) dtype_bytes = 4;
+  carve_workspace(op, n, d, n0, k, n_bins, n_offsets, dtype_bytes, nullptr, 0, &ws);
+  return ws.total;
+}
+
+int ggp_read_status(const void* workspace, ggp_status_t* out, ggp_stream_t stream) {
+  if (!workspace || !out) return GGP_ERR_INVALID;
+  DeviceStatus st;
+  cudaError_t e = cudaMemcpyAsync(&st, workspace, sizeof(st), cudaMemcpyDeviceToHost, GGP_STREAM(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(GGP_STREAM(stream));
+  if (e != cudaSuccess) return cuda_status(e);
+  out->error = st.error;
+  out->nan_seen = st.nan_seen;
+  out->fallback_count = st.fallback_count;
+  out->timeouts = st.timeouts;
+  return GGP_OK;
+}
+
+int ggp_refine_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                   const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals, int n_bins,
+                   const float* initial_values, const float* xi, float* out_values, double tau, uint64_t timeout_ns,
+                   void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return refine_impl<float>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                            initial_values, xi, out_values, tau, timeout_ns, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_refine_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                   const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals, int n_bins,
+                   const double* initial_values, const double* xi, double* out_values, uint64_t timeout_ns,
+                   void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return refine_impl<double>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                             initial_values, xi, out_values, 0.0, timeout_ns, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_refine_inv_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                       const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals, int n_bins,
+                       const float* values, float* out_initial_values, float* out_xi, double tau, void* workspace,
+                       size_t workspace_bytes, ggp_stream_t stream) {
+  return refine_inv_impl<float>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins, values,
+                                out_initial_values, out_xi, tau, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_refine_inv_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                       const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals,
+                       int n_bins, const double* values, double* out_initial_values, double* out_xi, void* workspace,
+                       size_t workspace_bytes, ggp_stream_t stream) {
+  return refine_inv_impl<double>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins, values,
+                                 out_initial_values, out_xi, 0.0, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_refine_logdet_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                          const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals,
+                          int n_bins, double* out_logdet, double tau, void* workspace, size_t workspace_bytes,
+                          ggp_stream_t stream) {
+  return refine_logdet_impl<float>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                                   out_logdet, tau, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_refine_logdet_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                          const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals,
+                          int n_bins, double* out_logdet, void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return refine_logdet_impl<double>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                                    out_logdet, 0.0, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_dense_f32(int mode, const float* points, int64_t n0, int d, const float* cov_bins, const float* cov_vals,
+                  int n_bins, const float* in, float* out, double* out_logdet, void* workspace, size_t workspace_bytes,
+                  ggp_stream_t stream) {
+  return dense_impl<float>(mode, points, n0, d, cov_bins, cov_vals, n_bins, in, out, out_logdet, workspace,
+                           workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_dense_f64(int mode, const double* points, int64_t n0, int d, const double* cov_bins, const double* cov_vals,
+                  int n_bins, const double* in, double* out, double* out_logdet, void* workspace,
+                  size_t workspace_bytes, ggp_stream_t stream) {
+  return dense_impl<double>(mode, points, n0, d, cov_bins, cov_vals, n_bins, in, out, out_logdet, workspace,
+                            workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                     const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const float* cov_bins,
+                     const float* cov_vals, int n_bins, const float* xi, float* out_values, double tau,
+                     uint64_t timeout_ns, void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return generate_impl<float>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                              xi, out_values, tau, timeout_ns, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                     const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const double* cov_bins,
+                     const double* cov_vals, int n_bins, const double* xi, double* out_values, uint64_t timeout_ns,
+                     void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return generate_impl<double>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                               xi, out_values, 0.0, timeout_ns, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_inv_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const float* cov_bins,
+                         const float* cov_vals, int n_bins, const float* values, float* out_xi, double tau,
+                         void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return generate_inv_impl<float>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
+                                  n_bins, values, out_xi, tau, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_inv_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                         const double* cov_bins, const double* cov_vals, int n_bins, const double* values,
+                         double* out_xi, void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return generate_inv_impl<double>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
+                                   n_bins, values, out_xi, 0.0, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_logdet_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                            const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals,
+                            int n_bins, double* out_logdet, double tau, void* workspace, size_t workspace_bytes,
+                            ggp_stream_t stream) {
+  return generate_logdet_impl<float>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                                     out_logdet, tau, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_logdet_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                            const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals,
+                            int n_bins, double* out_logdet, void* workspace, size_t workspace_bytes,
+                            ggp_stream_t stream) {
+  return generate_logdet_impl<double>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                                      out_logdet, 0.0, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+
+}  // extern "C"

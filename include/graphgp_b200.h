@@ -1,0 +1,246 @@
+/*
+ * graphgp_b200 -- C ABI of the B200 (sm_100a) kernels for GraphGP's graph build and conditional refinement.
+ *
+ * Each entry point replaces one function of the native extension that stanford-ism/graphgp calls behind
+ * its `cuda=True` switch (`import graphgp_cuda`, graphgp/tree.py:10-15, graph.py:12-17, refine.py:13-18),
+ * or one dense-root step that the reference runs through jnp.linalg. The cited line is the reference call
+ * site whose arguments and results the function reproduces.
+ *
+ * Conventions
+ *   - All array arguments are DEVICE pointers; nothing is done in place unless stated.
+ *   - Ids / indices / depths / offsets are int32. Points are row-major (n, d).
+ *   - `_f32` functions compute in FP32 (with FP64 where stated), `_f64` functions in FP64.
+ *   - Work is enqueued on `stream`; the call returns without synchronising.
+ *   - Every call takes a caller-owned device workspace of at least `ggp_workspace_size(...)` bytes,
+ *     256-byte aligned. Its first 256 bytes are a status block that device code fills (see
+ *     ggp_read_status); nothing else in it needs to survive between calls.
+ *   - Return value: GGP_OK or an error code for problems detectable on the host (bad sizes, workspace
+ *     too small, launch failure). Failures only the device can see (a bounded wait that ran out, NaN
+ *     results) are recorded in the status block and, like the reference (refine.py:55, 182), surface as
+ *     NaN outputs.
+ */
+#ifndef GRAPHGP_B200_H_
+#define GRAPHGP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* ggp_stream_t; /* same type as cudaStream_t */
+
+enum {
+  GGP_OK = 0,
+  GGP_ERR_INVALID = 1,     /* bad argument (shape, null pointer, n0 < k, unsorted offsets, ...) */
+  GGP_ERR_CUDA = 2,        /* a CUDA launch or runtime call failed */
+  GGP_ERR_TIMEOUT = 3,     /* a bounded device wait ran out (reported through the status block) */
+  GGP_ERR_UNSUPPORTED = 4, /* size outside what this build handles (e.g. k > 236, > 65536 bins) */
+  GGP_ERR_WORKSPACE = 5    /* workspace smaller than ggp_workspace_size */
+};
+
+/* Operation ids for ggp_workspace_size. */
+enum {
+  GGP_OP_BUILD_TREE = 1,
+  GGP_OP_QUERY_NEIGHBORS = 2,
+  GGP_OP_BUILD_GRAPH = 3,
+  GGP_OP_COMPUTE_DEPTHS = 4,
+  GGP_OP_ORDER_BY_DEPTH = 5,
+  GGP_OP_REFINE = 6,
+  GGP_OP_REFINE_INV = 7,
+  GGP_OP_REFINE_LOGDET = 8,
+  GGP_OP_GENERATE = 9,
+  GGP_OP_GENERATE_INV = 10,
+  GGP_OP_GENERATE_LOGDET = 11,
+  GGP_OP_DENSE = 12,
+  GGP_OP_GENERATE_VJP = 13
+};
+
+typedef struct {
+  uint32_t error;          /* GGP_* code recorded by device code, 0 if none */
+  uint32_t nan_seen;       /* an output contained NaN */
+  uint32_t fallback_count; /* points re-conditioned in FP64 because a pivot ratio fell below tau */
+  uint32_t timeouts;       /* bounded waits that ran out */
+} ggp_status_t;
+
+/* Library version string, e.g. "graphgp_b200 0.1.0 sm_100a". */
+const char* ggp_version(void);
+
+/* Bytes of workspace an operation needs. Arguments that do not apply to `op` are ignored. */
+size_t ggp_workspace_size(int op, int64_t n, int d, int64_t n0, int k, int n_bins, int n_offsets, int dtype_bytes);
+
+/* Copy the status block of a workspace to the host (synchronises `stream`). */
+int ggp_read_status(const void* workspace, ggp_status_t* out, ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Graph build (reference graphgp/tree.py, graphgp/graph.py)                                       */
+/* ---------------------------------------------------------------------------------------------- */
+
+/* graphgp_cuda.build_tree(points) -- graphgp/tree.py:37 (semantics tree.py:153-234).
+ * out_points (n, d) in tree order, out_split_dims (n,), out_indices (n,) original index of each. */
+int ggp_build_tree_f32(const float* points, int64_t n, int d, float* out_points, int32_t* out_split_dims,
+                       int32_t* out_indices, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_build_tree_f64(const double* points, int64_t n, int d, double* out_points, int32_t* out_split_dims,
+                       int32_t* out_indices, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* graphgp_cuda.query_preceding_neighbors(points, split_dims, n0=, k=) -- graphgp/tree.py:61
+ * (semantics tree.py:41-63, 79-150). out_neighbors (n - n0, k), sorted by (distance, index). */
+int ggp_query_preceding_neighbors_f32(const float* points, const int32_t* split_dims, int64_t n, int d,
+                                      int64_t n0, int k, int32_t* out_neighbors, void* workspace,
+                                      size_t workspace_bytes, ggp_stream_t stream);
+int ggp_query_preceding_neighbors_f64(const double* points, const int32_t* split_dims, int64_t n, int d,
+                                      int64_t n0, int k, int32_t* out_neighbors, void* workspace,
+                                      size_t workspace_bytes, ggp_stream_t stream);
+
+/* graphgp_cuda.query_neighbors(points, split_dims, query_indices, max_indices, k=) -- graphgp/tree.py:73.
+ * Query q searches tree nodes < max_indices[q]. out_neighbors (n_queries, k). */
+int ggp_query_neighbors_f32(const float* points, const int32_t* split_dims, int64_t n, int d,
+                            const int32_t* query_indices, const int32_t* max_indices, int64_t n_queries, int k,
+                            int32_t* out_neighbors, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_query_neighbors_f64(const double* points, const int32_t* split_dims, int64_t n, int d,
+                            const int32_t* query_indices, const int32_t* max_indices, int64_t n_queries, int k,
+                            int32_t* out_neighbors, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* graphgp_cuda.compute_depths_parallel(neighbors, n0=) -- graphgp/graph.py:106 (semantics 101-120).
+ * out_depths (n,) with n = n0 + rows of neighbors. */
+int ggp_compute_depths(const int32_t* neighbors, int64_t n, int64_t n0, int k, int32_t* out_depths,
+                       void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* graphgp_cuda.order_by_depth(points, indices, neighbors, depths) -- graphgp/graph.py:128 (semantics
+ * 123-137). Stable sort by depth; neighbour ids remapped. Also writes the batch offsets
+ * (graph.py:95-96) to out_offsets (capacity n + 1) and their count to *out_n_offsets (device int32). */
+int ggp_order_by_depth_f32(const float* points, const int32_t* indices, const int32_t* neighbors,
+                           const int32_t* depths, int64_t n, int d, int64_t n0, int k, float* out_points,
+                           int32_t* out_indices, int32_t* out_neighbors, int32_t* out_depths, int32_t* out_offsets,
+                           int32_t* out_n_offsets, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_order_by_depth_f64(const double* points, const int32_t* indices, const int32_t* neighbors,
+                           const int32_t* depths, int64_t n, int d, int64_t n0, int k, double* out_points,
+                           int32_t* out_indices, int32_t* out_neighbors, int32_t* out_depths, int32_t* out_offsets,
+                           int32_t* out_n_offsets, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* graphgp_cuda.build_graph(points, n0=, k=) -- graphgp/graph.py:89: tree, preceding k-NN, depths,
+ * ordering. Outputs as ggp_order_by_depth (offsets included). */
+int ggp_build_graph_f32(const float* points, int64_t n, int d, int64_t n0, int k, float* out_points,
+                        int32_t* out_indices, int32_t* out_neighbors, int32_t* out_depths, int32_t* out_offsets,
+                        int32_t* out_n_offsets, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_build_graph_f64(const double* points, int64_t n, int d, int64_t n0, int k, double* out_points,
+                        int32_t* out_indices, int32_t* out_neighbors, int32_t* out_depths, int32_t* out_offsets,
+                        int32_t* out_n_offsets, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Refinement (reference graphgp/refine.py)                                                        */
+/* `offsets` is the reference's offsets tuple as a device array (refine.py:120): n_offsets entries,   */
+/* offsets[0] = n0, offsets[n_offsets-1] = n; n0 = n - rows(neighbors) (refine.py:111). `tau`: a point whose smallest pivot ratio              */
+/* (Schur complement / variance) falls below tau is re-conditioned in FP64 (f32 functions only;       */
+/* 0 disables). `timeout_ns` bounds every wait of a point on a neighbour value (0 = default 10 s).   */
+/* ---------------------------------------------------------------------------------------------- */
+
+/* graphgp_cuda.refine(points, neighbors, offsets, cov_bins, cov_vals, initial_values, xi) --
+ * graphgp/refine.py:119-121 (semantics 123-159). out_values (n,) in graph order. */
+int ggp_refine_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k, const int32_t* offsets,
+                   int n_offsets, const float* cov_bins, const float* cov_vals, int n_bins,
+                   const float* initial_values, const float* xi, float* out_values, double tau,
+                   uint64_t timeout_ns, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_refine_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k, const int32_t* offsets,
+                   int n_offsets, const double* cov_bins, const double* cov_vals, int n_bins,
+                   const double* initial_values, const double* xi, double* out_values, uint64_t timeout_ns,
+                   void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* graphgp_cuda.refine_inv(points, neighbors, offsets, cov_bins, cov_vals, values) --
+ * graphgp/refine.py:216-218 (semantics 219-231). out_initial_values (n0,), out_xi (n - n0,). */
+int ggp_refine_inv_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                       const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals,
+                       int n_bins, const float* values, float* out_initial_values, float* out_xi, double tau,
+                       void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_refine_inv_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                       const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals,
+                       int n_bins, const double* values, double* out_initial_values, double* out_xi,
+                       void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* graphgp_cuda.refine_logdet(points, neighbors, offsets, cov_bins, cov_vals) -- graphgp/refine.py:265
+ * (semantics 266-275). Sum of log std accumulated in FP64; *out_logdet is a device double. */
+int ggp_refine_logdet_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                          const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals,
+                          int n_bins, double* out_logdet, double tau, void* workspace, size_t workspace_bytes,
+                          ggp_stream_t stream);
+int ggp_refine_logdet_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                          const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals,
+                          int n_bins, double* out_logdet, void* workspace, size_t workspace_bytes,
+                          ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Dense root in FP64 (reference graphgp/refine.py:59-76, 186-195, 243-248: jnp.linalg.cholesky,     */
+/* L @ xi, solve(L, v), slogdet(K)/2). Points / xi / values in T, factorisation and sums in FP64.  */
+/* mode: 0 = generate (out = L xi), 1 = inverse (out = L^-1 v), 2 = logdet (*out_logdet = sum log L_ii) */
+/* ---------------------------------------------------------------------------------------------- */
+int ggp_dense_f32(int mode, const float* points, int64_t n0, int d, const float* cov_bins, const float* cov_vals,
+                  int n_bins, const float* in, float* out, double* out_logdet, void* workspace,
+                  size_t workspace_bytes, ggp_stream_t stream);
+int ggp_dense_f64(int mode, const double* points, int64_t n0, int d, const double* cov_bins,
+                  const double* cov_vals, int n_bins, const double* in, double* out, double* out_logdet,
+                  void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Whole-graph operations (reference graphgp/refine.py:21-56 generate, 162-183 generate_inv,         */
+/* 234-240 generate_logdet): permutation by `indices` (may be NULL), FP64 dense root, refinement,    */
+/* scatter back, NaN poisoning -- all on the device in one call.                                     */
+/* ---------------------------------------------------------------------------------------------- */
+int ggp_generate_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0, const int32_t* neighbors,
+                     int k, const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals,
+                     int n_bins, const float* xi, float* out_values, double tau, uint64_t timeout_ns,
+                     void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_generate_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0, const int32_t* neighbors,
+                     int k, const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals,
+                     int n_bins, const double* xi, double* out_values, uint64_t timeout_ns, void* workspace,
+                     size_t workspace_bytes, ggp_stream_t stream);
+int ggp_generate_inv_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                         const float* cov_bins, const float* cov_vals, int n_bins, const float* values,
+                         float* out_xi, double tau, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_generate_inv_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                         const double* cov_bins, const double* cov_vals, int n_bins, const double* values,
+                         double* out_xi, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_generate_logdet_f32(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                            const int32_t* offsets, int n_offsets, const float* cov_bins, const float* cov_vals,
+                            int n_bins, double* out_logdet, double tau, void* workspace, size_t workspace_bytes,
+                            ggp_stream_t stream);
+int ggp_generate_logdet_f64(const double* points, int64_t n, int d, int64_t n0, const int32_t* neighbors, int k,
+                            const int32_t* offsets, int n_offsets, const double* cov_bins,
+                            const double* cov_vals, int n_bins, double* out_logdet, void* workspace,
+                            size_t workspace_bytes, ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Adjoint of generate (the custom_vjp the reference README promises for its CUDA primitives,         */
+/* README.md:36; JAX autodiff of graphgp/refine.py:21-76,123-145 on the pure-JAX path).                */
+/* Given xi (n,) and cotangent g_values (n,) (both in the caller's original point order), and a       */
+/* scalar cotangent g_logdet for generate_logdet, writes                                            */
+/*   out_grad_xi (n,)        = d/dxi  <g_values, generate(xi)>                                       */
+/*   out_grad_vals (n_bins,) = d/dcov_vals [<g_values, generate(xi)> + g_logdet * generate_logdet]   */
+/* out_grad_vals is FP64. Per-point Cholesky factors are recomputed, never stored.                   */
+/* ---------------------------------------------------------------------------------------------- */
+int ggp_generate_vjp_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                         const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
+                         const float* g_values, double g_logdet, float* out_grad_xi, double* out_grad_vals,
+                         double tau, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                         const double* cov_bins, const double* cov_vals, int n_bins, const double* xi,
+                         const double* g_values, double g_logdet, double* out_grad_xi, double* out_grad_vals,
+                         void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Failure-detection probe: launches one kernel whose single wait watches a flag that nothing sets,  */
+/* bounded by timeout_ns; returns GGP_ERR_TIMEOUT in *out_code (host int) when the bound worked.      */
+/* Synchronises `stream`. No counterpart in the reference (its only device failure signal is NaN).  */
+/* ---------------------------------------------------------------------------------------------- */
+int ggp_wait_probe(uint64_t timeout_ns, int* out_code, void* workspace, size_t workspace_bytes,
+                   ggp_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAPHGP_B200_H_ */
