@@ -1,0 +1,269 @@
+// Preceding k-nearest-neighbour query over the implicit k-d tree (reference graphgp/tree.py:41-150).
+//
+// One thread per query runs the reference's stack-free traversal verbatim: start at the root, "visit"
+// a node when arriving from its parent (tree.py:121-123), go to the near child first, take the far child
+// only if it exists (< max_index) and split_distance^2 <= radius^2 (inclusive, tree.py:129-136), climb
+// to the parent otherwise. A visit replaces the FIRST slot holding the largest squared distance iff the
+// new squared distance is strictly smaller (tree.py:84-91); the radius is the largest slot value. The
+// result is ordered by (sqrt(d2), index) (tree.py:103-104). Squared distances are summed left to right
+// over dimensions with unfused, round-to-nearest operations so the ids match the oracle bit for bit.
+//
+// Node records pack the point and its split dim into one 16-byte (float) / 32-byte (double) load.
+#pragma once
+
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace ggp {
+
+template <typename T> struct alignas(4 * sizeof(T)) NodeRec { T x, y, z, s; };
+
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rn_sqrt(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double rn_sqrt(double a) { return __dsqrt_rn(a); }
+
+template <typename T>
+__global__ void pack_nodes_kernel(const T* __restrict__ points, const int* __restrict__ split, long long n, int d,
+                                  NodeRec<T>* __restrict__ rec) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    NodeRec<T> r;
+    r.x = points[i * d];
+    r.y = d > 1 ? points[i * d + 1] : T(0);
+    r.z = d > 2 ? points[i * d + 2] : T(0);
+    r.s = (T)split[i];
+    rec[i] = r;
+  }
+}
+
+// Point access: packed records for d <= 3, strided rows for larger d.
+template <typename T, int D>
+struct PointSource {
+  const NodeRec<T>* rec;
+  const T* points;
+  const int* split;
+  int d;
+  __device__ __forceinline__ void load(long long i, T* p, int& s) const {
+    if (D > 0) {
+      const NodeRec<T> r = rec[i];
+      p[0] = r.x;
+      if (D > 1) p[1] = r.y;
+      if (D > 2) p[2] = r.z;
+      s = (int)r.s;
+    } else {
+      for (int c = 0; c < d; ++c) p[c] = points[i * d + c];
+      s = split[i];
+    }
+  }
+};
+
+template <typename T, int D>
+__device__ __forceinline__ T sqdist(const T* a, const T* b, int d) {
+  const int dd = D > 0 ? D : d;
+  T df = rn_sub(a[0], b[0]);
+  T acc = rn_mul(df, df);
+  for (int c = 1; c < dd; ++c) {
+    df = rn_sub(a[c], b[c]);
+    acc = rn_add(acc, rn_mul(df, df));
+  }
+  return acc;
+}
+
+template <typename T, int D>
+__device__ __forceinline__ T coord(const T* p, int s) {
+  if (D == 1) return p[0];
+  if (D == 2) return s == 0 ? p[0] : p[1];
+  if (D == 3) return s == 0 ? p[0] : (s == 1 ? p[1] : p[2]);
+  return p[s];
+}
+
+constexpr int kKnnMaxD = 16;
+
+// KMAX: compile-time slot capacity (registers for KMAX <= 32); k <= KMAX at run time.
+// Queries: query_idx / max_idx arrays, or (when null) rows q0 + t with max index = the row itself.
+template <typename T, int D, int KMAX>
+__global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long long n, int k,
+                                                  const int* __restrict__ query_idx, const int* __restrict__ max_idx,
+                                                  long long nq, long long q0, int* __restrict__ out) {
+  constexpr int PD = D > 0 ? D : kKnnMaxD;
+  const T inf = (T)INFINITY;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += (long long)gridDim.x * blockDim.x) {
+    long long qi = query_idx ? (long long)query_idx[t] : q0 + t;
+    qi = qi < 0 ? 0 : (qi >= n ? n - 1 : qi);  // out-of-range query ids clamp like a JAX gather
+    long long mx = max_idx ? (long long)max_idx[t] : qi;
+    if (mx > n) mx = n;
+    T q[PD];
+    int qs;
+    src.load(qi, q, qs);
+    int nb[KMAX];
+    T dv[KMAX];
+#pragma unroll
+    for (int j = 0; j < KMAX; ++j) {
+      nb[j] = -1;
+      dv[j] = (j < k) ? inf : (T)-1;  // inactive slots are never the largest
+    }
+    T maxv = inf;
+    int maxj = 0;
+    long long cur = mx > 0 ? 0 : -1, prev = -1;
+    while (cur != -1) {
+      const long long par = tree_parent(cur);
+      T p[PD];
+      int s;
+      src.load(cur, p, s);
+      if (prev == par) {
+        const T d2 = sqdist<T, D>(q, p, src.d);
+        if (d2 < maxv) {
+#pragma unroll
+          for (int j = 0; j < KMAX; ++j)
+            if (j == maxj) { nb[j] = (int)cur; dv[j] = d2; }
+          maxv = dv[0];
+          maxj = 0;
+#pragma unroll
+          for (int j = 1; j < KMAX; ++j)
+            if (dv[j] > maxv) { maxv = dv[j]; maxj = j; }
+        }
+      }
+      const T sd = rn_sub(coord<T, D>(q, s), coord<T, D>(p, s));
+      const int lvl = 63 - __clzll(cur + 1);
+      const long long left = cur + (1ll << lvl), right = cur + (2ll << lvl);
+      const long long nearc = sd < T(0) ? left : right;
+      const long long farc = sd < T(0) ? right : left;
+      const bool far_in = rn_mul(sd, sd) <= maxv;
+      long long next;
+      if (prev == nearc || (prev == par && nearc >= mx)) next = (farc < mx && far_in) ? farc : par;
+      else next = (prev == par) ? nearc : par;
+      prev = cur;
+      cur = next;
+    }
+    // order by (sqrt(d2), index); an unfilled slot (-1) measures against the last point like the
+    // reference's points[-1] gather (tree.py:103)
+    T key[KMAX];
+#pragma unroll
+    for (int j = 0; j < KMAX; ++j) {
+      if (j < k) {
+        T dd = dv[j];
+        if (nb[j] < 0) {
+          T p[PD];
+          int s;
+          src.load(n - 1, p, s);
+          dd = sqdist<T, D>(p, q, src.d);
+        }
+        key[j] = rn_sqrt(dd);
+      } else {
+        key[j] = inf;
+        nb[j] = 0x7fffffff;
+      }
+    }
+    // odd-even transposition sort (KMAX passes) on (key, id)
+#pragma unroll
+    for (int pass = 0; pass < KMAX; ++pass) {
+#pragma unroll
+      for (int j = (pass & 1); j + 1 < KMAX; j += 2) {
+        const bool sw = (key[j + 1] < key[j]) || (key[j + 1] == key[j] && nb[j + 1] < nb[j]);
+        if (sw) {
+          const T tk = key[j]; key[j] = key[j + 1]; key[j + 1] = tk;
+          const int ti = nb[j]; nb[j] = nb[j + 1]; nb[j + 1] = ti;
+        }
+      }
+    }
+    int* o = out + t * k;
+#pragma unroll
+    for (int j = 0; j < KMAX; ++j)
+      if (j < k) o[j] = nb[j];
+  }
+}
+
+}  // namespace ggp
+
+namespace ggp {
+
+// Same traversal for k > 32 (slots in local memory, loops not unrolled).
+constexpr int kKnnMaxK = 256;
+
+template <typename T, int D>
+__global__ void __launch_bounds__(128) knn_kernel_wide(PointSource<T, D> src, long long n, int k,
+                                                       const int* __restrict__ query_idx,
+                                                       const int* __restrict__ max_idx, long long nq, long long q0,
+                                                       int* __restrict__ out) {
+  constexpr int PD = D > 0 ? D : kKnnMaxD;
+  const T inf = (T)INFINITY;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += (long long)gridDim.x * blockDim.x) {
+    long long qi = query_idx ? (long long)query_idx[t] : q0 + t;
+    qi = qi < 0 ? 0 : (qi >= n ? n - 1 : qi);
+    long long mx = max_idx ? (long long)max_idx[t] : qi;
+    if (mx > n) mx = n;
+    T q[PD];
+    int qs;
+    src.load(qi, q, qs);
+    int nb[kKnnMaxK];
+    T dv[kKnnMaxK];
+#pragma unroll 1
+    for (int j = 0; j < k; ++j) { nb[j] = -1; dv[j] = inf; }
+    T maxv = inf;
+    int maxj = 0;
+    long long cur = mx > 0 ? 0 : -1, prev = -1;
+    while (cur != -1) {
+      const long long par = tree_parent(cur);
+      T p[PD];
+      int s;
+      src.load(cur, p, s);
+      if (prev == par) {
+        const T d2 = sqdist<T, D>(q, p, src.d);
+        if (d2 < maxv) {
+          nb[maxj] = (int)cur;
+          dv[maxj] = d2;
+          maxv = dv[0];
+          maxj = 0;
+#pragma unroll 1
+          for (int j = 1; j < k; ++j)
+            if (dv[j] > maxv) { maxv = dv[j]; maxj = j; }
+        }
+      }
+      const T sd = rn_sub(coord<T, D>(q, s), coord<T, D>(p, s));
+      const int lvl = 63 - __clzll(cur + 1);
+      const long long left = cur + (1ll << lvl), right = cur + (2ll << lvl);
+      const long long nearc = sd < T(0) ? left : right;
+      const long long farc = sd < T(0) ? right : left;
+      const bool far_in = rn_mul(sd, sd) <= maxv;
+      long long next;
+      if (prev == nearc || (prev == par && nearc >= mx)) next = (farc < mx && far_in) ? farc : par;
+      else next = (prev == par) ? nearc : par;
+      prev = cur;
+      cur = next;
+    }
+#pragma unroll 1
+    for (int j = 0; j < k; ++j) {
+      T dd = dv[j];
+      if (nb[j] < 0) {
+        T p[PD];
+        int s;
+        src.load(n - 1, p, s);
+        dd = sqdist<T, D>(p, q, src.d);
+      }
+      dv[j] = rn_sqrt(dd);
+    }
+    // insertion sort on (distance, id)
+#pragma unroll 1
+    for (int i = 1; i < k; ++i) {
+      const T kv = dv[i];
+      const int ki = nb[i];
+      int j = i - 1;
+      while (j >= 0 && (kv < dv[j] || (kv == dv[j] && ki < nb[j]))) {
+        dv[j + 1] = dv[j];
+        nb[j + 1] = nb[j];
+        --j;
+      }
+      dv[j + 1] = kv;
+      nb[j + 1] = ki;
+    }
+    int* o = out + t * k;
+#pragma unroll 1
+    for (int j = 0; j < k; ++j) o[j] = nb[j];
+  }
+}
+
+}  // namespace ggp

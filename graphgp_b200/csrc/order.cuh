@@ -1,0 +1,220 @@
+// Depths, stable ordering by depth and batch offsets (reference graphgp/graph.py:95-137).
+#pragma once
+
+#include "common.cuh"
+
+namespace ggp {
+
+// depth[i] = 0 for i < n0, else 1 + max(depth[nbrs]) (graph.py:101-120: the Jacobi fixed point, which for a
+// topologically ordered graph is this single pass). Warps take chunks of 32 rows in row order; a row waits
+// (bounded) for neighbours before its chunk, which belong to earlier tickets; neighbours inside the chunk
+// are resolved by iterating max-plus updates over warp shuffles until nothing changes.
+__global__ void __launch_bounds__(256) depths_kernel(const int* __restrict__ nbrs, long long n, long long n0, int k,
+                                                     int* __restrict__ depth, DeviceStatus* st,
+                                                     unsigned long long timeout_ns) {
+  const int lane = threadIdx.x & 31;
+  const long long n_chunks = (n - n0 + 31) / 32;
+  for (;;) {
+    const unsigned int t = warp_ticket(&st->ticket);
+    if (t >= n_chunks) break;
+    const long long cs = n0 + (long long)t * 32;
+    const long long row = cs + lane;
+    const bool valid = row < n;
+    const int* nr = nbrs + (valid ? (row - n0) : 0) * k;
+    int ext = -1;
+    bool bad = false;
+    if (valid) {
+      for (int m = 0; m < k; ++m) {
+        const int id = nr[m];
+        if (id < 0 || (long long)id >= row) { bad = true; continue; }
+        if ((long long)id < cs) {
+          int v = ld_relaxed(depth + id);
+          if (v < 0) {
+            const uint64_t t0 = global_timer_ns();
+            unsigned int backoff = 32;
+            while (v < 0) {
+              __nanosleep(backoff);
+              if (backoff < 512) backoff <<= 1;
+              v = ld_relaxed(depth + id);
+              if (v < 0 && global_timer_ns() - t0 > timeout_ns) {
+                atomicAdd(&st->timeouts, 1u);
+                report_error(st, GGP_ERR_TIMEOUT);
+                v = 0;
+              }
+            }
+          }
+          ext = v > ext ? v : ext;
+        }
+      }
+    }
+    if (bad) report_error(st, GGP_ERR_INVALID);
+    int my = ext + 1;
+    for (int it = 0; it < 33; ++it) {
+      bool changed = false;
+      for (int m = 0; m < k; ++m) {
+        const int id = valid ? nr[m] : -1;
+        const bool inside = valid && (long long)id >= cs && (long long)id < row;
+        const int srcl = inside ? (int)(id - cs) : lane;
+        const int v = __shfl_sync(0xffffffffu, my, srcl);
+        if (inside && v + 1 > my) { my = v + 1; changed = true; }
+      }
+      if (!__any_sync(0xffffffffu, changed)) break;
+    }
+    if (valid) st_relaxed(depth + row, my);
+  }
+}
+
+__global__ void depths_init_kernel(int* __restrict__ depth, long long n, long long n0) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    depth[i] = i < n0 ? 0 : -1;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Stable LSD radix sort of (uint32 key, int32 value), 8-bit digits, 4096-element tiles.
+// ------------------------------------------------------------------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t* __restrict__ keys, long long n,
+                                                                  int shift, unsigned int* __restrict__ counts,
+                                                                  int n_tiles) {
+  __shared__ unsigned int h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * kSortTile;
+  for (int j = 0; j < kSortItems; ++j) {
+    const long long e = base + (long long)j * kSortThreads + threadIdx.x;
+    if (e < n) atomicAdd(&h[(keys[e] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  counts[(long long)threadIdx.x * n_tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of `m` counters in one block (digit-major order gives each (digit, tile) its base).
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(unsigned int* __restrict__ a, long long m) {
+  __shared__ unsigned long long s[1024];
+  const long long per = (m + blockDim.x - 1) / blockDim.x;
+  const long long lo = threadIdx.x * per, hi = min(m, lo + per);
+  unsigned long long local = 0;
+  for (long long i = lo; i < hi; ++i) local += a[i];
+  s[threadIdx.x] = local;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+    const unsigned long long v = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+    __syncthreads();
+    s[threadIdx.x] += v;
+    __syncthreads();
+  }
+  unsigned long long run = s[threadIdx.x] - local;
+  for (long long i = lo; i < hi; ++i) {
+    const unsigned int c = a[i];
+    a[i] = (unsigned int)run;
+    run += c;
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint32_t* __restrict__ kin,
+                                                                     const int* __restrict__ vin,
+                                                                     uint32_t* __restrict__ kout,
+                                                                     int* __restrict__ vout, long long n, int shift,
+                                                                     const unsigned int* __restrict__ counts,
+                                                                     int n_tiles) {
+  __shared__ unsigned int base[256];
+  __shared__ unsigned int running[256];
+  __shared__ unsigned int wc[kSortThreads / 32][257];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  base[tid] = counts[(long long)tid * n_tiles + blockIdx.x];
+  running[tid] = 0;
+  const unsigned int lt = (1u << lane) - 1u;
+  const long long tile = (long long)blockIdx.x * kSortTile;
+  for (int j = 0; j < kSortItems; ++j) {
+    for (int q = tid; q < (kSortThreads / 32) * 257; q += kSortThreads) (&wc[0][0])[q] = 0;
+    __syncthreads();
+    const long long e = tile + (long long)j * kSortThreads + tid;
+    const bool ok = e < n;
+    const uint32_t key = ok ? kin[e] : 0u;
+    const int val = ok ? vin[e] : 0;
+    const int dg = ok ? (int)((key >> shift) & 255u) : 256;
+    const unsigned int peers = __match_any_sync(0xffffffffu, dg);
+    const int rank = __popc(peers & lt);
+    if (rank == 0) wc[w][dg] = __popc(peers);
+    __syncthreads();
+    if (ok) {
+      unsigned int pre = 0;
+      for (int ww = 0; ww < w; ++ww) pre += wc[ww][dg];
+      const unsigned int pos = base[dg] + running[dg] + pre + rank;
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncthreads();
+    unsigned int tot = 0;
+    for (int ww = 0; ww < kSortThreads / 32; ++ww) tot += wc[ww][tid];
+    running[tid] += tot;
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// ordering by depth (graph.py:123-137)
+// ------------------------------------------------------------------------------------------------
+__global__ void iota_kernel(int* __restrict__ v, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = (int)i;
+}
+
+template <typename T>
+__global__ void order_gather_kernel(const int* __restrict__ perm, long long n, int d, const T* __restrict__ points,
+                                    const int* __restrict__ indices, T* __restrict__ out_points,
+                                    int* __restrict__ out_idx, int* __restrict__ inv) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long s = perm[i];
+    for (int c = 0; c < d; ++c) out_points[i * d + c] = points[s * d + c];
+    out_idx[i] = indices[s];
+    inv[s] = (int)i;
+  }
+}
+
+// neighbors = inv_order[neighbors[order[n0:] - n0]] (graph.py:131-136); one warp per row
+__global__ void order_neighbors_kernel(const int* __restrict__ perm, const int* __restrict__ inv,
+                                       const int* __restrict__ nbrs, long long n, long long n0, int k,
+                                       int* __restrict__ out_nbrs, DeviceStatus* st) {
+  const long long rows = n - n0;
+  const int lane = threadIdx.x & 31;
+  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += ((long long)gridDim.x * blockDim.x) >> 5) {
+    long long src = (long long)perm[n0 + r] - n0;
+    if (src < 0 || src >= rows) {  // a refined row ordered before n0 (depth 0): graph invalid
+      if (lane == 0) report_error(st, GGP_ERR_INVALID);
+      src = src < 0 ? 0 : rows - 1;
+    }
+    for (int m = lane; m < k; m += 32) {
+      int id = nbrs[src * k + m];
+      id = (id < 0) ? 0 : ((long long)id >= n ? (int)(n - 1) : id);  // gather clamps like JAX
+      out_nbrs[r * k + m] = inv[id];
+    }
+  }
+}
+
+// offsets[b] = first i with depth[i] > b, b = 0..max_depth (graph.py:95-96); count = max_depth + 1.
+__global__ void offsets_kernel(const uint32_t* __restrict__ sorted_depth, long long n, int* __restrict__ offsets,
+                               int* __restrict__ n_offsets) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x + 1; i <= n; i += (long long)gridDim.x * blockDim.x) {
+    const long long lo = sorted_depth[i - 1];
+    const long long hi = (i < n) ? (long long)sorted_depth[i] : lo + 1;
+    for (long long b = lo; b < hi; ++b) offsets[b] = (int)i;
+    if (i == n) *n_offsets = (int)(lo + 1);
+  }
+}
+
+__global__ void depth_copy_kernel(const int* __restrict__ depth, uint32_t* __restrict__ key, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    key[i] = (uint32_t)max(depth[i], 0);
+}
+
+__global__ void u32_to_i32_kernel(const uint32_t* __restrict__ a, int* __restrict__ b, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (int)a[i];
+}
+
+}  // namespace ggp

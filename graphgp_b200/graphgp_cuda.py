@@ -19,7 +19,7 @@ import torch
 
 from . import _lib
 
-DEFAULT_TAU = 1e-3
+DEFAULT_TAU = 1e-5
 """FP32 points whose smallest Cholesky pivot ratio (Schur complement / prior variance) falls below this
 threshold are re-conditioned in FP64."""
 

@@ -1,0 +1,53 @@
+"""CPU-side checks of the C-ABI library: it loads, and it exports every entry point include/graphgp_b200.h
+declares (no compute calls; those need a GPU)."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "graphgp_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|size_t|const char\*)\s+(ggp_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for base in ("build_tree", "query_preceding_neighbors", "query_neighbors", "compute_depths", "order_by_depth",
+                 "build_graph", "refine", "refine_inv", "refine_logdet"):
+        assert any(s.startswith("ggp_" + base) for s in syms), base
+
+
+def test_library_loads_and_exports_all_symbols():
+    from graphgp_b200 import _lib
+
+    path = _lib.lib_path()
+    if not path.exists():
+        pytest.fail(f"library not built: {path}")
+    lib = ctypes.CDLL(str(path))  # resolves every undefined symbol (RTLD_NOW below)
+    lib = ctypes.CDLL(str(path), mode=ctypes.RTLD_GLOBAL | 2)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(_lib.exported_symbols()) == set(declared_symbols())
+
+
+def test_version_and_workspace_size_without_gpu():
+    from graphgp_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.ggp_version().startswith(b"graphgp_b200")
+    sz = lib.ggp_workspace_size(_lib.OPS["GENERATE"], 1 << 20, 3, 1024, 16, 2049, 100, 4)
+    assert sz >= (1 << 20) * 4 + 1024 * 1024 * 8
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    from graphgp_b200 import _lib
+
+    monkeypatch.setattr(_lib, "_LIB_PATH", tmp_path / "absent.so")
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(ImportError):
+        _lib.load()
