@@ -1,0 +1,479 @@
+#!/usr/bin/env python
+"""Benchmark of the GraphGP hot path on B200: FP32 ``generate`` (FP64 dense root) at the precision-at-scale
+workload -- N = 16,777,216 points in d = 3 (unit direction x 10^U(-3, 0), float32, seed 99), n0 = 1024,
+k = 16, Matern-3/2 (variance 1, cutoff 0.05) tabulated at r = 0 plus 2048 log bins on [1e-6, 4],
+jitter 1e-5, xi ~ N(0, 1). The graph is built once on the GPU (untimed, reported separately); a step is
+one ``generate`` of all N points with the inputs resident in HBM (inputs larger than L2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n N]
+
+Prints one JSON line (rank 0). With --gpus N > 1 (torchrun) every rank runs an independent replica on its
+own GPU ("replicas only": generate has no shardable exchange step); value = all ranks' points / max time.
+``--impl reference`` times the CPU restatement of the reference's algorithm (the NumPy oracle) on the host
+cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "points/sec generate+grad, FP32 vs FP64 at ≤1e-4 rel err; p50/p99 request latency"
+WORKLOAD = dict(name="generate, precision at scale", n=1 << 24, d=3, n0=1024, k=16, kernel="matern-3/2",
+                cutoff=0.05, r_min=1e-6, r_max=4.0, n_bins=2049, jitter=1e-5, seed=99)
+BYTES_PER_POINT = 4 * WORKLOAD["k"] * (WORKLOAD["d"] + 2) + 4 * WORKLOAD["d"] + 8  # 340 B (k=16, d=3)
+
+
+def synth_points(n, d=3, seed=99):
+    """Unit direction times radius 10^U(-3, 0) (heavy dynamic range), float32."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal((n, d))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return (v * 10.0 ** rng.uniform(-3, 0, (n, 1))).astype(np.float32)
+
+
+def table():
+    from graphgp_b200 import extras
+
+    w = WORKLOAD
+    return extras.matern_kernel(p=1, variance=1.0, cutoff=w["cutoff"], r_min=w["r_min"], r_max=w["r_max"],
+                                n_bins=w["n_bins"], jitter=w["jitter"])
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks / throttle reasons in the background during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl" if _cuda_ok() else "gloo", timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def _cuda_ok():
+    import torch
+
+    return torch.cuda.is_available()
+
+
+def max_over_ranks(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------------------
+# FP64 comparators
+# ------------------------------------------------------------------------------------------------
+def fp64_fastjit_generate(P, I, NB, offsets, bins, vals, xi, chunk=1 << 19):
+    """The plain FP64-GPU form shaped like the reference's fast_jit path (refine.py:123-145): materialise
+    the (k+1)^2 covariance of every point in float64, batched Cholesky (torch / cuSOLVER), mean_vec =
+    solve(L11^T, l21), then the batch scan of gathers. Dense root in FP64 as well. Comparator only."""
+    import torch
+
+    n = P.shape[0]
+    n0 = n - NB.shape[0]
+    k = NB.shape[1]
+    P64 = P.double()
+    b64 = bins.double()
+    v64 = vals.double()
+
+    def interp(r):
+        i = torch.clamp(torch.searchsorted(b64, r, right=True), 1, len(b64) - 1)
+        x0, x1 = b64[i - 1], b64[i]
+        f0, f1 = v64[i - 1], v64[i]
+        f = f0 + (r - x0) / (x1 - x0) * (f1 - f0)
+        f = torch.where(r < b64[0], v64[0], f)
+        return torch.where(r > b64[-1], v64[-1], f)
+
+    mean_vec = torch.empty((n - n0, k), dtype=torch.float64, device=P.device)
+    std = torch.empty(n - n0, dtype=torch.float64, device=P.device)
+    for s in range(0, n - n0, chunk):
+        e = min(n - n0, s + chunk)
+        joint = torch.cat([P64[NB[s:e].long()], P64[n0 + s:n0 + e, None]], dim=1)
+        K = interp(torch.cdist(joint, joint))
+        L = torch.linalg.cholesky(K)
+        mean_vec[s:e] = torch.linalg.solve_triangular(L[:, :k, :k].transpose(1, 2), L[:, k, :k, None],
+                                                      upper=True)[..., 0]
+        std[s:e] = L[:, k, k]
+        del joint, K, L
+    xi64 = xi.double()[I.long()]
+    K0 = interp(torch.cdist(P64[:n0], P64[:n0]))
+    values = torch.zeros(n, dtype=torch.float64, device=P.device)
+    values[:n0] = torch.linalg.cholesky(K0) @ xi64[:n0]
+    NBl = NB.long()
+    for b in range(1, len(offsets)):
+        s, e = offsets[b - 1], offsets[b]
+        rows = slice(s - n0, e - n0)
+        values[s:e] = (mean_vec[rows] * values[NBl[rows]]).sum(1) + std[rows] * xi64[s:e]
+    out = torch.empty_like(values)
+    out[I.long()] = values
+    return out
+
+
+# ------------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+
+    from graphgp_b200 import _lib
+    from graphgp_b200 import graphgp_cuda as gc
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOAD
+    n = args.n or w["n"]
+    lib = _lib.load()
+    pts = synth_points(n, w["d"], w["seed"])
+    bins, vals = table()
+    P = torch.as_tensor(pts, device=dev)
+    B = torch.as_tensor(bins, dtype=torch.float32, device=dev)
+    V = torch.as_tensor(vals, dtype=torch.float32, device=dev)
+    xi_host = np.random.default_rng(w["seed"] + 1).standard_normal(n).astype(np.float32)
+    XI = torch.as_tensor(xi_host, device=dev)
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    # graph (one-time, untimed for the metric)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record()
+    gp, gi, gn, gd, offs = gc.build_graph(P, n0=w["n0"], k=w["k"], return_offsets=True)
+    e1.record()
+    torch.cuda.synchronize()
+    graph_ms = e0.elapsed_time(e1)
+    OF = torch.as_tensor(offs, dtype=torch.int32, device=dev)
+
+    step = lambda: gc.generate(gp, gi, gn, OF, B, V, XI)  # noqa: E731
+    for _ in range(args.warmup):
+        out = step()
+    torch.cuda.synchronize()
+    st = gc.last_status()
+    launches0 = lib.ggp_launch_count()
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        for _ in range(args.steps):
+            out = step()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+    launches = (lib.ggp_launch_count() - launches0) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+
+    # dominant kernel: the refinement kernel in generate mode (graphgp_cuda.refine = prologue + that kernel)
+    init = out[gi[: w["n0"]].long()].contiguous()
+    xr = XI[gi[w["n0"]:].long()].contiguous()
+    for _ in range(2):
+        gc.refine(gp, gn, OF, B, V, init, xr)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(args.steps):
+        gc.refine(gp, gn, OF, B, V, init, xr)
+    e1.record()
+    torch.cuda.synchronize()
+    kern_ms = e0.elapsed_time(e1) / args.steps
+
+    # end to end through the public API with host buffers: pinned xi in, values out
+    xi_pin = torch.from_numpy(xi_host).pin_memory()
+    out_pin = torch.empty(n, dtype=torch.float32).pin_memory()
+    for _ in range(2):
+        out_pin.copy_(gc.generate(gp, gi, gn, OF, B, V, xi_pin.to(dev, non_blocking=True)), non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(args.steps):
+        x_d = xi_pin.to(dev, non_blocking=True)
+        out_pin.copy_(gc.generate(gp, gi, gn, OF, B, V, x_d), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+
+    extra = {}
+    if rank == 0 and not args.quick:
+        extra = comparisons(args, dev, gp, gi, gn, offs, OF, B, V, XI, pts, bins, vals, out, ms)
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = BYTES_PER_POINT * (n - w["n0"]) / (kern_ms * 1e-3) / 1e9
+    traffic = read_traffic(n - w["n0"])
+    line = {
+        "metric": METRIC,
+        "value": n * world / (ms * 1e-3),
+        "unit": "points/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (FP64 dense root, FP64 logdet sums, FP64 re-conditioning below pivot ratio 1e-5)",
+        "data": "synthetic (seeded NumPy: unit direction x 10^U(-3,0), float32; xi N(0,1))",
+        "config": {"workload": w["name"], "n_points": n, "d": w["d"], "n0": w["n0"], "k": w["k"],
+                   "kernel": f"{w['kernel']} cutoff {w['cutoff']}, r=0 + {w['n_bins'] - 1} log bins on "
+                             f"[{w['r_min']}, {w['r_max']}], jitter {w['jitter']}",
+                   "batches": len(offs) - 1, "graph_build_ms": graph_ms, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (points 201 MB, neighbours 1.07 GB)"},
+        "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": "points/s",
+                "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_ms},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "kernel": "refine_quad_kernel<float,16,3> (generate mode)",
+                     "kernel_ms": kern_ms, "algorithmic_bytes_per_point": BYTES_PER_POINT,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+        "gpu_launches": launches,
+        "fallback_points": st["fallback_count"] if st else None,
+    }
+    line.update(extra)
+    if rank == 0:
+        line["clocks"] = clk.summary()
+        if not args.quick:
+            line["cpu_baseline"] = cpu_baseline(gp, gn, offs, bins, vals)
+        print(json.dumps(line), flush=True)
+
+
+def read_traffic(units):
+    """DRAM bytes per refined point of the dominant kernel from the committed ncu summary, scaled to one
+    launch; None when no capture has been summarised."""
+    path = os.path.join(ROOT, "profiles", "refine_quad_generate_c2.md")
+    try:
+        for ln in open(path):
+            if ln.startswith("dram_bytes_per_point:"):
+                return float(ln.split(":")[1]) * units
+    except OSError:
+        pass
+    return None
+
+
+def comparisons(args, dev, gp, gi, gn, offs, OF, B, V, XI, pts, bins, vals, out32, ms32):
+    """FP64 comparators on the full workload and the FP32-vs-FP64 error on a seed-matched 1M subset."""
+    import torch
+
+    from graphgp_b200 import graphgp_cuda as gc
+
+    res = {}
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    # (1) the same kernels instantiated in FP64
+    P64, B64, V64, X64 = gp.double(), torch.as_tensor(bins, device=dev), torch.as_tensor(vals, device=dev), XI.double()
+    out64 = gc.generate(P64, gi, gn, OF, B64, V64, X64)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(3):
+        out64 = gc.generate(P64, gi, gn, OF, B64, V64, X64)
+    e1.record()
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1) / 3
+    err = float(torch.linalg.vector_norm(out32.double() - out64) / torch.linalg.vector_norm(out64))
+    res["fp64_same_kernels"] = {"ms_per_step": ms64, "speedup_fp32": ms64 / ms32, "rel_err_fp32_vs_fp64": err}
+    del out64
+    # (2) plain FP64-GPU form shaped like the reference's fast_jit path
+    try:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ref = fp64_fastjit_generate(gp, gi, gn, offs, B64, V64, XI)
+        torch.cuda.synchronize()
+        msj = (time.perf_counter() - t0) * 1e3
+        errj = float(torch.linalg.vector_norm(out32.double() - ref) / torch.linalg.vector_norm(ref))
+        res["fp64_fastjit_form"] = {"ms_per_step": msj, "speedup_fp32": msj / ms32, "rel_err_fp32_vs_it": errj}
+        del ref
+    except RuntimeError as exc:  # out of memory etc.
+        res["fp64_fastjit_form"] = {"error": str(exc)[:200]}
+    torch.cuda.empty_cache()
+    # (3) error against FP64 on a seed-matched 1M-point subset (its own graph)
+    m = min(1 << 20, len(pts))
+    Ps = torch.as_tensor(pts[:m], device=dev)
+    sp, si, sn, sd, so = gc.build_graph(Ps, n0=WORKLOAD["n0"], k=WORKLOAD["k"], return_offsets=True)
+    xs = XI[:m].contiguous()
+    v32 = gc.generate(sp, si, sn, so, B, V, xs)
+    v64 = gc.generate(sp.double(), si, sn, so, B64, V64, xs.double())
+    res["subset_1m"] = {"rel_err": float(torch.linalg.vector_norm(v32.double() - v64) / torch.linalg.vector_norm(v64)),
+                        "max_abs_err": float((v32.double() - v64).abs().max())}
+    return res
+
+
+def cpu_baseline(gp, gn, offs, bins, vals, budget_s=12.0):
+    """The NumPy FP64 oracle's refine (reference refine.py:123-145 restated) timed on this host, one core,
+    on the first refined rows of the graph (a bounded sample of the same workload)."""
+    from oracle import refine as orf
+
+    n0 = WORKLOAD["n0"]
+    pts = gp.cpu().numpy().astype(np.float64)
+    rows = 0
+    chunk = 20000
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and rows < len(gn):
+        e = min(rows + chunk, gn.shape[0])
+        nb = gn[rows:e].cpu().numpy()
+        mv, sd = orf.factor_points(pts, nb, np.arange(n0 + rows, n0 + e), (bins, vals))
+        _ = np.sum(mv * pts[nb, 0], axis=1) + sd  # the value step (values of the sample's neighbours)
+        rows = e
+    dt = time.perf_counter() - t0
+    return {"value": rows / dt, "unit": "points/s", "cores": 1, "kind": "port",
+            "sample": f"first {rows} refined points of the workload graph (FP64 NumPy factorisation + value)"}
+
+
+# ------------------------------------------------------------------------------------------------
+# reference arm: the CPU restatement on all host cores
+# ------------------------------------------------------------------------------------------------
+def _ref_worker(payload):
+    pts, nb, rows0, bins, vals, n0 = payload
+    from oracle import refine as orf
+
+    mv, sd = orf.factor_points(pts, nb, np.arange(n0 + rows0, n0 + rows0 + len(nb)), (bins, vals))
+    return len(nb)
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    from oracle import graph as og
+
+    w = WORKLOAD
+    m = args.ref_sample
+    pts = synth_points(w["n"], w["d"], w["seed"])[:m].astype(np.float64)
+    bins, vals = table()
+    g = og.build_graph(pts, n0=w["n0"], k=w["k"])  # untimed, like our arm's graph
+    cores = os.cpu_count() or 1
+    parts = np.array_split(np.arange(len(g.neighbors)), cores * 2)
+    payloads = [(g.points, g.neighbors[p], int(p[0]), bins, vals, w["n0"]) for p in parts if len(p)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_worker, payloads[:cores])
+        t0 = time.perf_counter()
+        done = 0
+        for _ in range(args.steps):
+            done += sum(pool.map(_ref_worker, payloads))
+        dt = time.perf_counter() - t0
+    val = done / dt
+    print(json.dumps({
+        "metric": METRIC, "value": val, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (same generator, first "
+                                                       f"{m} points)",
+        "config": {"workload": w["name"], "n_points": w["n"], "d": w["d"], "n0": w["n0"], "k": w["k"],
+                   "sample_points": m},
+        "impl": "reference",
+        "cpu_baseline": {"value": val, "unit": "points/s", "cores": cores, "kind": "port",
+                         "sample": f"refinement of a {m}-point graph of the workload per step (NumPy FP64 oracle)"},
+        "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=0, help="override the number of points (testing)")
+    ap.add_argument("--quick", action="store_true", help="skip the FP64 comparators and CPU baseline")
+    ap.add_argument("--ref-sample", type=int, default=200000)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -10,6 +10,10 @@ namespace ggp {
 
 constexpr int kWarp = 32;
 
+// Host-side count of kernel launches made by this library (every launch site is wrapped as
+// `(count_launch(), kernel<<<...>>>(...))`); read through ggp_launch_count().
+void count_launch();
+
 template <typename T>
 __host__ __device__ __forceinline__ T ceil_div(T a, T b) { return (a + b - 1) / b; }
 

@@ -220,11 +220,11 @@ __global__ void dense_logdet_kernel(const double* __restrict__ L, long long n0, 
 inline cudaError_t dense_cholesky(double* A, long long n0, cudaStream_t s) {
   const int nt = (int)((n0 + kDenseTile - 1) / kDenseTile);
   for (int p = 0; p < nt; ++p) {
-    dense_potrf_tile_kernel<<<1, 256, 0, s>>>(A, n0, p);
+    (ggp::count_launch(), dense_potrf_tile_kernel<<<1, 256, 0, s>>>(A, n0, p));
     const int below = nt - p - 1;
     if (below > 0) {
-      dense_trsm_kernel<<<below, kDenseTile, 0, s>>>(A, n0, p);
-      dense_update_kernel<<<below * (below + 1) / 2, 256, 0, s>>>(A, n0, p, nt);
+      (ggp::count_launch(), dense_trsm_kernel<<<below, kDenseTile, 0, s>>>(A, n0, p));
+      (ggp::count_launch(), dense_update_kernel<<<below * (below + 1) / 2, 256, 0, s>>>(A, n0, p, nt));
     }
   }
   return cudaGetLastError();

@@ -156,7 +156,7 @@ static int build_tree_device(const T* points, long long n, int d, T* out_points,
                              char* scratch, DeviceStatus* st, cudaStream_t s) {
   TreeWs<T> w;
   tree_ws_bytes<T>(n, d, &w, scratch);
-  tree_init_kernel<T><<<g_grid(n), 256, 0, s>>>(points, n, d, w.soa[0], w.idx[0]);
+  (ggp::count_launch(), tree_init_kernel<T><<<g_grid(n), 256, 0, s>>>(points, n, d, w.soa[0], w.idx[0]));
   int cur = 0;
   const int L = bit_length(n);
   for (int l = 0; l < L; ++l) {
@@ -167,28 +167,28 @@ static int build_tree_device(const T* points, long long n, int d, T* out_points,
     if (smax > kSegA) {
       const int cps = (int)((smax + kChunkA - 1) / kChunkA);
       const long long grid = Lv.n_level * cps;
-      box_init_kernel<<<g_grid(Lv.n_level * d * 2), 256, 0, s>>>(w.box, Lv.n_level * d * 2);
-      tree_bbox_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, d, n, w.soa[cur], w.box);
-      tree_split_kernel<T><<<g_grid(Lv.n_level), 256, 0, s>>>(Lv, d, w.box, w.st, out_split);
+      (ggp::count_launch(), box_init_kernel<<<g_grid(Lv.n_level * d * 2), 256, 0, s>>>(w.box, Lv.n_level * d * 2));
+      (ggp::count_launch(), tree_bbox_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, d, n, w.soa[cur], w.box));
+      (ggp::count_launch(), tree_split_kernel<T><<<g_grid(Lv.n_level), 256, 0, s>>>(Lv, d, w.box, w.st, out_split));
       cudaMemsetAsync(w.hist, 0, sizeof(unsigned int) * (size_t)Lv.n_level * kBins, s);
       for (int p = 0; p < n_passes<KeyType<T>::BITS>(); ++p) {
-        tree_hist_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, n, w.soa[cur], w.st, p, w.hist);
-        tree_pick_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, w.st, p, w.hist);
+        (ggp::count_launch(), tree_hist_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, n, w.soa[cur], w.st, p, w.hist));
+        (ggp::count_launch(), tree_pick_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, w.st, p, w.hist));
       }
-      tree_tie_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, n, w.soa[cur], w.idx[cur], w.st, out_split);
+      (ggp::count_launch(), tree_tie_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, n, w.soa[cur], w.idx[cur], w.st, out_split));
       cudaMemsetAsync(w.cursor, 0, sizeof(unsigned long long) * (size_t)(2 * Lv.n_level), s);
-      tree_partition_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, N1, cps, d, n, w.soa[cur], w.idx[cur], w.soa[cur ^ 1],
+      (ggp::count_launch(), tree_partition_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, N1, cps, d, n, w.soa[cur], w.idx[cur], w.soa[cur ^ 1],
                                                               w.idx[cur ^ 1], w.st, out_split, w.cursor, out_points,
-                                                              out_idx, st);
+                                                              out_idx, st));
       cur ^= 1;
     } else if (smax > kSegC || d > 8) {
-      tree_block_level_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, N1, d, n, w.soa[cur], w.idx[cur], w.soa[cur ^ 1],
-                                                                       w.idx[cur ^ 1], out_split, out_points, out_idx, st);
+      (ggp::count_launch(), tree_block_level_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, N1, d, n, w.soa[cur], w.idx[cur], w.soa[cur ^ 1],
+                                                                       w.idx[cur ^ 1], out_split, out_points, out_idx, st));
       cur ^= 1;
     } else {
       const long long threads = Lv.n_level * 32;
-      tree_leaf_kernel<T><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(Lv, d, n, w.soa[cur], w.idx[cur], out_split,
-                                                                            out_points, out_idx, st);
+      (ggp::count_launch(), tree_leaf_kernel<T><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(Lv, d, n, w.soa[cur], w.idx[cur], out_split,
+                                                                            out_points, out_idx, st));
       break;
     }
     cudaError_t e = cudaGetLastError();
@@ -204,10 +204,10 @@ template <typename T, int D>
 static cudaError_t launch_knn_d(const PointSource<T, D>& src, long long n, int k, const int* q, const int* m,
                                 long long nq, long long q0, int* out, cudaStream_t s) {
   const int grid = g_grid(nq, 128);
-  if (k <= 8) knn_kernel<T, D, 8><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out);
-  else if (k <= 16) knn_kernel<T, D, 16><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out);
-  else if (k <= 32) knn_kernel<T, D, 32><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out);
-  else knn_kernel_wide<T, D><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out);
+  if (k <= 8) (ggp::count_launch(), knn_kernel<T, D, 8><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+  else if (k <= 16) (ggp::count_launch(), knn_kernel<T, D, 16><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+  else if (k <= 32) (ggp::count_launch(), knn_kernel<T, D, 32><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+  else (ggp::count_launch(), knn_kernel_wide<T, D><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
   return cudaGetLastError();
 }
 
@@ -219,7 +219,7 @@ static int knn_device(const T* points, const int* split, long long n, int d, int
   knn_ws_bytes<T>(n, &rec, scratch);
   cudaError_t e;
   if (d <= 3) {
-    pack_nodes_kernel<T><<<g_grid(n), 256, 0, s>>>(points, split, n, d, rec);
+    (ggp::count_launch(), pack_nodes_kernel<T><<<g_grid(n), 256, 0, s>>>(points, split, n, d, rec));
     if (d == 1) e = launch_knn_d<T, 1>(PointSource<T, 1>{rec, points, split, d}, n, k, q, m, nq, q0, out, s);
     else if (d == 2) e = launch_knn_d<T, 2>(PointSource<T, 2>{rec, points, split, d}, n, k, q, m, nq, q0, out, s);
     else e = launch_knn_d<T, 3>(PointSource<T, 3>{rec, points, split, d}, n, k, q, m, nq, q0, out, s);
@@ -234,14 +234,14 @@ static int knn_device(const T* points, const int* split, long long n, int d, int
 // ------------------------------------------------------------------------------------------------
 static int depths_device(const int* nbrs, long long n, long long n0, int k, int* depth, DeviceStatus* st,
                          cudaStream_t s) {
-  depths_init_kernel<<<g_grid(n), 256, 0, s>>>(depth, n, n0);
+  (ggp::count_launch(), depths_init_kernel<<<g_grid(n), 256, 0, s>>>(depth, n, n0));
   if (n > n0) {
     int per_sm = 0, sms = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, depths_kernel, 256, 0);
     if (per_sm < 1) per_sm = 1;
-    depths_kernel<<<sms * per_sm, 256, 0, s>>>(nbrs, n, n0, k, depth, st, 10000000000ull);
+    (ggp::count_launch(), depths_kernel<<<sms * per_sm, 256, 0, s>>>(nbrs, n, n0, k, depth, st, 10000000000ull));
   }
   return g_status(cudaGetLastError());
 }
@@ -253,21 +253,21 @@ static int order_device(const T* points, const int* indices, const int* nbrs, co
   OrderWs w;
   order_ws_bytes(n, &w, scratch);
   const int tiles = (int)((n + kSortTile - 1) / kSortTile);
-  depth_copy_kernel<<<g_grid(n), 256, 0, s>>>(depths, w.key[0], n);
-  iota_kernel<<<g_grid(n), 256, 0, s>>>(w.val[0], n);
+  (ggp::count_launch(), depth_copy_kernel<<<g_grid(n), 256, 0, s>>>(depths, w.key[0], n));
+  (ggp::count_launch(), iota_kernel<<<g_grid(n), 256, 0, s>>>(w.val[0], n));
   const int bits = bit_length(n - n0 + 1);  // depths never exceed n - n0
   int cur = 0;
   for (int shift = 0; shift < bits; shift += 8) {
-    radix_hist_kernel<<<tiles, kSortThreads, 0, s>>>(w.key[cur], n, shift, w.counts, tiles);
-    exclusive_scan_kernel<<<1, 1024, 0, s>>>(w.counts, (long long)tiles * 256);
-    radix_scatter_kernel<<<tiles, kSortThreads, 0, s>>>(w.key[cur], w.val[cur], w.key[cur ^ 1], w.val[cur ^ 1], n, shift,
-                                                        w.counts, tiles);
+    (ggp::count_launch(), radix_hist_kernel<<<tiles, kSortThreads, 0, s>>>(w.key[cur], n, shift, w.counts, tiles));
+    (ggp::count_launch(), exclusive_scan_kernel<<<1, 1024, 0, s>>>(w.counts, (long long)tiles * 256));
+    (ggp::count_launch(), radix_scatter_kernel<<<tiles, kSortThreads, 0, s>>>(w.key[cur], w.val[cur], w.key[cur ^ 1], w.val[cur ^ 1], n, shift,
+                                                        w.counts, tiles));
     cur ^= 1;
   }
-  order_gather_kernel<T><<<g_grid(n), 256, 0, s>>>(w.val[cur], n, d, points, indices, out_points, out_idx, w.inv);
-  order_neighbors_kernel<<<g_grid((n - n0) * 32), 256, 0, s>>>(w.val[cur], w.inv, nbrs, n, n0, k, out_nbrs, st);
-  u32_to_i32_kernel<<<g_grid(n), 256, 0, s>>>(w.key[cur], out_depths, n);
-  if (out_offsets) offsets_kernel<<<g_grid(n), 256, 0, s>>>(w.key[cur], n, out_offsets, out_n_offsets);
+  (ggp::count_launch(), order_gather_kernel<T><<<g_grid(n), 256, 0, s>>>(w.val[cur], n, d, points, indices, out_points, out_idx, w.inv));
+  (ggp::count_launch(), order_neighbors_kernel<<<g_grid((n - n0) * 32), 256, 0, s>>>(w.val[cur], w.inv, nbrs, n, n0, k, out_nbrs, st));
+  (ggp::count_launch(), u32_to_i32_kernel<<<g_grid(n), 256, 0, s>>>(w.key[cur], out_depths, n));
+  if (out_offsets) (ggp::count_launch(), offsets_kernel<<<g_grid(n), 256, 0, s>>>(w.key[cur], n, out_offsets, out_n_offsets));
   return g_status(cudaGetLastError());
 }
 

@@ -1,9 +1,14 @@
 // Failure-detection probe: one kernel whose only wait watches a flag that nothing ever sets. The bounded
 // wait must give up after `timeout_ns`, record GGP_ERR_TIMEOUT in the status block and return, leaving
 // the context usable. Used by the tests to exercise the same wait_ready() the refinement kernels use.
+#include <atomic>
+
 #include "common.cuh"
 
 namespace ggp {
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 __global__ void wait_probe_kernel(const float* flag, DeviceStatus* st, unsigned long long timeout_ns) {
   float v;
@@ -25,8 +30,8 @@ extern "C" int ggp_wait_probe(uint64_t timeout_ns, int* out_code, void* workspac
   DeviceStatus* st = (DeviceStatus*)workspace;
   float* flag = (float*)((char*)workspace + 256);
   cudaMemsetAsync(st, 0, sizeof(DeviceStatus), s);
-  fill_pending_probe_kernel<<<1, 1, 0, s>>>(flag);
-  wait_probe_kernel<<<1, 1, 0, s>>>(flag, st, timeout_ns ? timeout_ns : 1000000ull);
+  (ggp::count_launch(), fill_pending_probe_kernel<<<1, 1, 0, s>>>(flag));
+  (ggp::count_launch(), wait_probe_kernel<<<1, 1, 0, s>>>(flag, st, timeout_ns ? timeout_ns : 1000000ull));
   DeviceStatus h;
   cudaError_t e = cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -34,3 +39,5 @@ extern "C" int ggp_wait_probe(uint64_t timeout_ns, int* out_code, void* workspac
   *out_code = (int)h.error;
   return GGP_OK;
 }
+
+extern "C" uint64_t ggp_launch_count(void) { return ggp::g_launches.load(std::memory_order_relaxed); }

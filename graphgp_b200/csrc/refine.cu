@@ -14,7 +14,7 @@ namespace ggp {
 // small helper kernels
 // ------------------------------------------------------------------------------------------------
 
-// chunk_prefix[b] = chunks (32 rows each) in batches before b; validates the offsets array.
+// chunk_prefix[b] = chunks (chunk_rows() rows each) in batches before b; validates the offsets array.
 __global__ void chunk_prefix_kernel(const int* __restrict__ offsets, int n_offsets, long long n0, long long n,
                                     int* __restrict__ prefix, DeviceStatus* st) {
   __shared__ long long s_sum[1024];
@@ -27,7 +27,7 @@ __global__ void chunk_prefix_kernel(const int* __restrict__ offsets, int n_offse
   for (int b = b0; b < b1; ++b) {
     const long long a = offsets[b], c = offsets[b + 1];
     if (c < a) bad = true;
-    local += (c > a) ? (c - a + 31) / 32 : 0;
+    local += (c > a) ? (c - a + chunk_rows(c - a) - 1) / chunk_rows(c - a) : 0;
   }
   s_sum[threadIdx.x] = local;
   __syncthreads();
@@ -41,7 +41,7 @@ __global__ void chunk_prefix_kernel(const int* __restrict__ offsets, int n_offse
   for (int b = b0; b < b1; ++b) {
     prefix[b] = (int)run;
     const long long a = offsets[b], c = offsets[b + 1];
-    run += (c > a) ? (c - a + 31) / 32 : 0;
+    run += (c > a) ? (c - a + chunk_rows(c - a) - 1) / chunk_rows(c - a) : 0;
   }
   if (threadIdx.x == blockDim.x - 1) prefix[nbatch] = (int)s_sum[threadIdx.x];
   if (threadIdx.x == 0) {
@@ -160,7 +160,7 @@ inline int cuda_status(cudaError_t e) {
 
 template <typename TB>
 cudaError_t prepare_table(const TB* bins, const TB* vals, int nb, const TableBuffers& tb, cudaStream_t s) {
-  prepare_table_kernel<TB><<<1, 256, 0, s>>>(bins, vals, nb, tb);
+  (ggp::count_launch(), prepare_table_kernel<TB><<<1, 256, 0, s>>>(bins, vals, nb, tb));
   return cudaGetLastError();
 }
 
@@ -201,7 +201,7 @@ int run_logdet(RefineParams<T> p, int nb, double* out, const double* add, cudaSt
     cudaError_t e = dispatch<T>(p, kLogdet, nb, kMaxPartials, s);
     if (e != cudaSuccess) return cuda_status(e);
   }
-  sum_partials_kernel<<<1, 1024, 0, s>>>(p.logdet_partials, kMaxPartials, add, out);
+  (ggp::count_launch(), sum_partials_kernel<<<1, 1024, 0, s>>>(p.logdet_partials, kMaxPartials, add, out));
   return cuda_status(cudaGetLastError());
 }
 
@@ -210,8 +210,8 @@ template <typename T>
 int prologue(const Workspace& ws, const T* bins, const T* vals, int nb, const int* offsets, int n_offsets,
              long long n0, long long n, cudaStream_t s) {
   cudaMemsetAsync(ws.status, 0, sizeof(DeviceStatus), s);
-  prepare_table_kernel<T><<<1, 256, 0, s>>>(bins, vals, nb, ws.table);
-  if (n_offsets >= 1 && offsets) chunk_prefix_kernel<<<1, 1024, 0, s>>>(offsets, n_offsets, n0, n, ws.chunk_prefix, ws.status);
+  (ggp::count_launch(), prepare_table_kernel<T><<<1, 256, 0, s>>>(bins, vals, nb, ws.table));
+  if (n_offsets >= 1 && offsets) (ggp::count_launch(), chunk_prefix_kernel<<<1, 1024, 0, s>>>(offsets, n_offsets, n0, n, ws.chunk_prefix, ws.status));
   return cuda_status(cudaGetLastError());
 }
 
@@ -239,15 +239,15 @@ int dense_root(const Workspace& ws, const T* points, long long n0, int d, int mo
     if (mode == 2) { cudaMemsetAsync(out_logdet, 0, sizeof(double), s); }
     return cuda_status(cudaGetLastError());
   }
-  dense_cov_kernel<T><<<grid_for(n0 * n0), 256, 0, s>>>(points, n0, d, nullptr, ws.table, ws.dense);
+  (ggp::count_launch(), dense_cov_kernel<T><<<grid_for(n0 * n0), 256, 0, s>>>(points, n0, d, nullptr, ws.table, ws.dense));
   cudaError_t e = dense_cholesky(ws.dense, n0, s);
   if (e != cudaSuccess) return cuda_status(e);
   if (mode == 0) {
-    dense_matvec_kernel<T><<<grid_for(n0 * 32), 256, 0, s>>>(ws.dense, n0, in, perm, out_graph, out_user, ws.status);
+    (ggp::count_launch(), dense_matvec_kernel<T><<<grid_for(n0 * 32), 256, 0, s>>>(ws.dense, n0, in, perm, out_graph, out_user, ws.status));
   } else if (mode == 1) {
-    dense_trsv_kernel<T><<<1, 1024, 0, s>>>(ws.dense, n0, in, perm, ws.dense_x, out_graph, out_user, ws.status);
+    (ggp::count_launch(), dense_trsv_kernel<T><<<1, 1024, 0, s>>>(ws.dense, n0, in, perm, ws.dense_x, out_graph, out_user, ws.status));
   } else {
-    dense_logdet_kernel<<<1, 1024, 0, s>>>(ws.dense, n0, out_logdet);
+    (ggp::count_launch(), dense_logdet_kernel<<<1, 1024, 0, s>>>(ws.dense, n0, out_logdet));
   }
   return cuda_status(cudaGetLastError());
 }
@@ -272,7 +272,7 @@ int refine_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nb
   rc = carve_workspace(GGP_OP_REFINE, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
   if (rc) return rc;
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
-  init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(out, init, n0, n, offsets, n_offsets);
+  (ggp::count_launch(), init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(out, init, n0, n, offsets, n_offsets));
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, timeout_ns);
   p.values = out;
   p.xi = xi;
@@ -290,7 +290,7 @@ int refine_inv_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t
   rc = carve_workspace(GGP_OP_REFINE_INV, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
   if (rc) return rc;
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
-  if (n0 > 0) copy_kernel<T><<<grid_for(n0), 256, 0, s>>>(values, out_init, n0);
+  if (n0 > 0) (ggp::count_launch(), copy_kernel<T><<<grid_for(n0), 256, 0, s>>>(values, out_init, n0));
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
   p.values = const_cast<T*>(values);
   p.xi_out = out_xi;
@@ -322,7 +322,7 @@ int dense_impl(int mode, const T* points, int64_t n0, int d, const T* bins, cons
   int rc = carve_workspace(GGP_OP_DENSE, n0, d, n0, 1, nb, 1, sizeof(T), wsp, ws_bytes, &ws);
   if (rc) return rc;
   cudaMemsetAsync(ws.status, 0, sizeof(DeviceStatus), s);
-  prepare_table_kernel<T><<<1, 256, 0, s>>>(bins, vals, nb, ws.table);
+  (ggp::count_launch(), prepare_table_kernel<T><<<1, 256, 0, s>>>(bins, vals, nb, ws.table));
   return dense_root<T>(ws, points, n0, d, mode, in, nullptr, out, nullptr, out_logdet, s);
 }
 
@@ -339,7 +339,7 @@ int generate_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
   T* vg = (T*)ws.values_graph;
   // rows >= n0 pending (rows past the last offset 0); rows < n0 come from the dense root below
-  init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, nullptr, n0, n, offsets, n_offsets);
+  (ggp::count_launch(), init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, nullptr, n0, n, offsets, n_offsets));
   if ((rc = dense_root<T>(ws, points, n0, d, 0, xi, perm, vg, out, nullptr, s))) return rc;
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, timeout_ns);
   p.values = vg;
@@ -352,8 +352,8 @@ int generate_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_
     p.xi = xi + n0;
   }
   if ((rc = run_cond<T>(p, kGenerate, nb, s))) return rc;
-  if (!perm) copy_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, out, n);
-  poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out, n, ws.status);
+  if (!perm) (ggp::count_launch(), copy_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, out, n));
+  (ggp::count_launch(), poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out, n, ws.status));
   return cuda_status(cudaGetLastError());
 }
 
@@ -369,7 +369,7 @@ int generate_inv_impl(const T* points, const int32_t* perm, int64_t n, int d, in
   if (rc) return rc;
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
   T* vg = (T*)ws.values_graph;
-  gather_kernel<T><<<grid_for(n), 256, 0, s>>>(values, perm, vg, n);  // values in graph order
+  (ggp::count_launch(), gather_kernel<T><<<grid_for(n), 256, 0, s>>>(values, perm, vg, n));  // values in graph order
   // dense part: xi[:n0] = L^-1 v[:n0] (refine.py:186-195), gathered from / scattered to user order
   if ((rc = dense_root<T>(ws, points, n0, d, 1, values, perm, nullptr, out_xi, nullptr, s))) return rc;
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
@@ -378,7 +378,7 @@ int generate_inv_impl(const T* points, const int32_t* perm, int64_t n, int d, in
   p.out_user = perm ? out_xi : nullptr;
   p.xi_out = perm ? nullptr : out_xi + n0;
   if ((rc = run_cond<T>(p, kInverse, nb, s))) return rc;
-  poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out_xi, n, ws.status);
+  (ggp::count_launch(), poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out_xi, n, ws.status));
   return cuda_status(cudaGetLastError());
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "refine_generic.cuh"
+#include "refine_quad.cuh"
 
 namespace ggp {
 
@@ -19,15 +20,15 @@ template <typename T, int K, int D, bool PAD>
 cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_blocks, cudaStream_t s) {
   const size_t smem = table_smem_bytes<T>(nb);
   if (kind == kCond) {
-    auto kern = refine_cond_kernel<T, K, D, PAD>;
+    auto kern = refine_quad_kernel<T, K, D, PAD, false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int grid = persistent_grid(kern, 128, smem, max_blocks);
-    kern<<<grid, 128, smem, s>>>(p);
+    (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));
   } else {
-    auto kern = refine_logdet_kernel<T, K, D, PAD>;
+    auto kern = refine_quad_kernel<T, K, D, PAD, true>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int grid = persistent_grid(kern, 128, smem, max_blocks);
-    kern<<<grid, 128, smem, s>>>(p);
+    (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));
   }
   return cudaGetLastError();
 }
@@ -40,7 +41,7 @@ cudaError_t launch_generic(const RefineParams<T>& p, int kind, int max_blocks, c
   if (e != cudaSuccess) return e;
   const int grid = persistent_grid(kern, 128, smem, max_blocks);
   const int mode = (kind == kLogdet) ? 2 : p.mode;
-  kern<<<grid, 128, smem, s>>>(p, mode);
+  (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p, mode));
   return cudaGetLastError();
 }
 #endif

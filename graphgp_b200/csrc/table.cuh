@@ -32,7 +32,9 @@ struct TableDesc {
   double b0, v0, blast, vlast;
   double c0;          // cov_lookup(0): the diagonal of every covariance matrix
   int sorted;         // 1 if bins are non-decreasing
-  int pad[3];
+  int max_steps32;    // most forward steps a float lookup can need from its hint cell
+  int max_steps64;    // same for double lookups
+  int pad;
 };
 
 // Workspace layout of a prepared table (all offsets 256-byte aligned by the caller).
@@ -109,19 +111,21 @@ __global__ void prepare_table_kernel(const TB* __restrict__ bins, const TB* __re
     while (jp < nb - 1 && !((double)bins[jp] > 0.0)) ++jp;
     double bpos = (double)bins[jp] > 0.0 ? (double)bins[jp] : 1e-30;
     double blast = (double)bins[nb - 1] > bpos ? (double)bins[nb - 1] : bpos;
-    int sh32 = 23 - 8, sh64 = 52 - 8;
-    long long lo32 = (long long)(__float_as_uint((float)bpos) >> sh32);
+    // finest cells (up to 2^10 per octave) whose count fits kHintMax; cell 0 lies entirely below the first
+    // positive bin, so every radius under it starts from bracket 0
+    int sh32 = 23 - 10, sh64 = 52 - 10;
+    long long lo32 = (long long)(__float_as_uint((float)bpos) >> sh32) - 1;
     long long hi32 = (long long)(__float_as_uint((float)blast) >> sh32);
     while (hi32 - lo32 + 1 > kHintMax) {
       ++sh32;
-      lo32 = (long long)(__float_as_uint((float)bpos) >> sh32);
+      lo32 = (long long)(__float_as_uint((float)bpos) >> sh32) - 1;
       hi32 = (long long)(__float_as_uint((float)blast) >> sh32);
     }
-    long long lo64 = (long long)((unsigned long long)__double_as_longlong(bpos) >> sh64);
+    long long lo64 = (long long)((unsigned long long)__double_as_longlong(bpos) >> sh64) - 1;
     long long hi64 = (long long)((unsigned long long)__double_as_longlong(blast) >> sh64);
     while (hi64 - lo64 + 1 > kHintMax) {
       ++sh64;
-      lo64 = (long long)((unsigned long long)__double_as_longlong(bpos) >> sh64);
+      lo64 = (long long)((unsigned long long)__double_as_longlong(bpos) >> sh64) - 1;
       hi64 = (long long)((unsigned long long)__double_as_longlong(blast) >> sh64);
     }
     int nh = (int)((hi32 - lo32 + 1) > (hi64 - lo64 + 1) ? (hi32 - lo32 + 1) : (hi64 - lo64 + 1));
@@ -172,6 +176,25 @@ __global__ void prepare_table_kernel(const TB* __restrict__ bins, const TB* __re
     tb.hint32[c] = h32;
     tb.hint64[c] = h64;
   }
+  __syncthreads();
+  // most forward steps any radius needs from its cell's hint: the brackets that start inside one cell
+  __shared__ int s_steps32, s_steps64;
+  if (threadIdx.x == 0) { s_steps32 = 0; s_steps64 = 0; }
+  __syncthreads();
+  int m32 = 0, m64 = 0;
+  for (int c = threadIdx.x; c < nh; c += blockDim.x) {
+    const int n32 = (c + 1 < nh) ? (int)tb.hint32[c + 1] : bracket_search(bins, nb, (double)bins[nb - 1]);
+    const int n64 = (c + 1 < nh) ? (int)tb.hint64[c + 1] : bracket_search(bins, nb, (double)bins[nb - 1]);
+    m32 = max(m32, n32 - (int)tb.hint32[c]);
+    m64 = max(m64, n64 - (int)tb.hint64[c]);
+  }
+  atomicMax(&s_steps32, m32);
+  atomicMax(&s_steps64, m64);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tb.desc->max_steps32 = s_steps32 + 1;
+    tb.desc->max_steps64 = s_steps64 + 1;
+  }
 }
 
 // Lookup against a table staged in shared memory (or global memory for the FP64 fallback).
@@ -182,18 +205,28 @@ struct TableView {
   long long key_lo;
   int shift;
   int n_hint;
-  int last;  // nb - 2
+  int last;       // nb - 2
+  int max_steps;  // forward steps a lookup may need from its hint (<= 2 on the straight-line path)
   T b0, v0, blast, vlast;
 
+  // Radii are clamped into [bins[0], bins[-1]]: below bins[0] the bracket-0 formula gives vals[0] exactly,
+  // above bins[-1] the last bracket gives vals[-1] up to one rounding (jnp.interp's end values).
   __device__ __forceinline__ T operator()(T r) const {
-    if (!(r > b0)) return v0;  // also r == b0 (interp gives vals[0]) and NaN-free distances
-    if (r > blast) return vlast;
+    r = fmin(fmax(r, b0), blast);
     long long c = radius_key(r, shift) - key_lo;
-    int j = 0;
-    if (c >= 0) j = hint[c < n_hint ? c : n_hint - 1];
+    c = c < 0 ? 0 : (c >= n_hint ? n_hint - 1 : c);
+    int j = hint[c];
     Bracket<T> e = br[j];
-    while (j < last && r >= e.b1) { ++j; e = br[j]; }
-    return e.v + (r - e.b) * e.s;
+    if (max_steps <= 2) {
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const bool step = (r >= e.b1) && (j < last);
+        if (step) { ++j; e = br[j]; }
+      }
+    } else {
+      while (j < last && r >= e.b1) { ++j; e = br[j]; }
+    }
+    return fma(r - e.b, e.s, e.v);
   }
 };
 
@@ -215,6 +248,7 @@ __device__ __forceinline__ TableView<T> global_table_view(const TableBuffers& tb
   v.shift = sizeof(T) == 4 ? d.shift32 : d.shift64;
   v.n_hint = d.n_hint;
   v.last = d.nb - 2;
+  v.max_steps = sizeof(T) == 4 ? d.max_steps32 : d.max_steps64;
   v.b0 = (T)d.b0; v.v0 = (T)d.v0; v.blast = (T)d.blast; v.vlast = (T)d.vlast;
   return v;
 }

@@ -70,6 +70,10 @@ const char* ggp_version(void);
 /* Bytes of workspace an operation needs. Arguments that do not apply to `op` are ignored. */
 size_t ggp_workspace_size(int op, int64_t n, int d, int64_t n0, int k, int n_bins, int n_offsets, int dtype_bytes);
 
+/* Number of kernel launches this library has made in the process so far (diagnostic; no counterpart in
+ * the reference). */
+uint64_t ggp_launch_count(void);
+
 /* Copy the status block of a workspace to the host (synchronises `stream`). */
 int ggp_read_status(const void* workspace, ggp_status_t* out, ggp_stream_t stream);
 

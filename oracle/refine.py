@@ -77,6 +77,18 @@ def generate_dense_logdet(points, covariance):
 # ------------------------------------------------------------------------------------------------
 # per-point factorisation (refine.py:130-135, 221-227, 269-273)
 # ------------------------------------------------------------------------------------------------
+def factor_points(points, nbr_rows, self_idx, covariance):
+    """mean_vec and std for points ``self_idx`` with neighbour id rows ``nbr_rows`` (see factor_rows)."""
+    points = np.asarray(points, np.float64)
+    nb = np.asarray(nbr_rows)
+    k = nb.shape[1]
+    joint = np.concatenate([points[nb], points[np.asarray(self_idx)][:, None, :]], axis=1)
+    K = compute_cov_matrix(covariance, joint, joint)
+    L = np.linalg.cholesky(K)
+    mean_vec = np.linalg.solve(np.transpose(L[:, :k, :k], (0, 2, 1)), L[:, k, :k][..., None])[..., 0]
+    return mean_vec, L[:, k, k]
+
+
 def factor_rows(points, neighbors, covariance, n0, rows):
     """For refined rows ``rows`` (0-based into ``neighbors``): joint = [nbr_0..nbr_{k-1}, self];
     K = cov(joint, joint); L = chol(K); mean_vec = solve(L11^T, l21); std = L[k, k]."""
