@@ -164,4 +164,4 @@ def test_interp_matches_numpy():
     """cov_lookup restates jnp.interp: equal to np.interp inside the table and clamped outside."""
     bins, vals = ox.rbf_kernel(variance=1.0, scale=0.3, r_min=1e-4, r_max=10, n_bins=1001, jitter=1e-4)
     r = np.concatenate([[0.0, 1e-5, 1e-4, 10.0, 11.0], np.random.default_rng(3).uniform(0, 12, 1000)])
-    assert np.allclose(orf.cov_lookup(r, bins, vals), np.interp(r, bins, vals), rtol=1e-14, atol=1e-300)
+    assert np.allclose(orf.cov_lookup(r, bins, vals), np.interp(r, bins, vals), rtol=1e-12, atol=1e-15)
