@@ -29,6 +29,7 @@ struct RefineParams {
   TableBuffers tb;
   DeviceStatus* status;
   double tau;               // FP64 re-conditioning threshold on the pivot ratio (0 disables)
+  int table_smem;           // bytes of dynamic shared memory taken by the staged table (256-aligned)
   unsigned long long timeout_ns;
 };
 

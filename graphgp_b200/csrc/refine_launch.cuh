@@ -18,6 +18,19 @@ cudaError_t launch_generic(const RefineParams<T>& p, int kind, int max_blocks, c
 #ifdef GGP_DEFINE_LAUNCHERS
 template <typename T, int K, int D, bool PAD>
 cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_blocks, cudaStream_t s) {
+  if constexpr (K <= 20) {
+    RefineParams<T> q = p;
+    q.table_smem = (int)((table_smem_bytes<T>(nb) + 255) / 256 * 256);
+    constexpr int kBlock = 256;
+    const size_t smem = q.table_smem + sizeof(T) * (kBlock / 32) * 8 * QuadSmem<K, D>::kPerPoint;
+    auto kern = (kind == kCond) ? refine_quad2_kernel<T, K, D, PAD, false> : refine_quad2_kernel<T, K, D, PAD, true>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int grid = persistent_grid(kern, kBlock, smem, 0);
+    if (max_blocks > 0 && grid > max_blocks) grid = max_blocks;
+    (ggp::count_launch(), kern<<<grid, kBlock, smem, s>>>(q));
+    return cudaGetLastError();
+  }
   const size_t smem = table_smem_bytes<T>(nb);
   if (kind == kCond) {
     auto kern = refine_quad_kernel<T, K, D, PAD, false>;

@@ -267,4 +267,215 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
   }
 }
 
+
+// ------------------------------------------------------------------------------------------------
+// Two-phase variant (k <= 20): the quad first evaluates the k(k+1)/2 off-diagonal covariances of the
+// point's neighbourhood into shared memory, dealt evenly over its four lanes (pair p -> lane p % 4, a
+// compact loop), then runs the same shuffle-broadcast left-looking factorisation reading its initial
+// entries from there. Compared with evaluating covariances inside the factorisation (where a lane only
+// evaluates its own rows and the quad waits for the busiest lane), this balances the table lookups,
+// removes their predication and keeps the unrolled code small.
+// ------------------------------------------------------------------------------------------------
+template <int K, int D> struct QuadSmem {
+  static constexpr int kPairs = K * (K + 1) / 2;             // rows 1..K, columns below the diagonal
+  static constexpr int kPointStride = (D <= 2 ? 2 : 4);     // coordinates per point slot
+  static constexpr int kPerPoint = (K + 1) * kPointStride + kPairs + 1;  // +1 staggers banks
+};
+
+template <typename T, int K, bool WITH_V>
+__device__ __forceinline__ void quad_condition_tri(const T* __restrict__ tri, const T (&val)[(K + 2 + kQuad - 1) / kQuad],
+                                                   int g, int src0, T c0, T& mean, T& var, T& min_ratio) {
+  constexpr int R = WITH_V ? K + 2 : K + 1;
+  constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
+  T L[NT][K + 1];
+#pragma unroll
+  for (int t = 0; t < NT; ++t)
+#pragma unroll
+    for (int m = 0; m <= K; ++m) L[t][m] = T(0);
+  T mr = T(1);
+  const T inv_c0 = T(1) / c0;
+  T mean_acc = T(0);
+  T var_out = T(0);
+#pragma unroll
+  for (int j = 0; j <= K; ++j) {
+    const int o = j % kQuad;
+    const int tj = j / kQuad;
+    const int src = src0 + o;
+    T vj = T(0);
+    if (WITH_V && j < K) vj = __shfl_sync(0xffffffffu, val[tj], src);
+    T acc[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int i = t * kQuad + g;
+      T a = T(0);
+      if (t * kQuad + kQuad - 1 >= j) {
+        if (i == j) a = c0;
+        else if (i > j && i <= K) a = tri[i * (i - 1) / 2 + j];
+        else if (WITH_V && i == K + 1) a = vj;
+      }
+      acc[t] = a;
+    }
+#pragma unroll
+    for (int m = 0; m < j; ++m) {
+      const T b = __shfl_sync(0xffffffffu, L[tj][m], src);
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+        if (t * kQuad + kQuad - 1 >= j) acc[t] = fma(-L[t][m], b, acc[t]);
+    }
+    const T s = __shfl_sync(0xffffffffu, acc[tj], src);
+    mr = fmin(mr, s * inv_c0);
+    if (j == K) var_out = s;
+    const T r = fast_rsqrt<T>(s);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int i = t * kQuad + g;
+      if (WITH_V && j == K && i == K + 1) mean_acc = -acc[t];
+      if (t * kQuad + kQuad - 1 >= j) L[t][j] = (i > j && i < R) ? acc[t] * r : L[t][j];
+    }
+  }
+  mean = mean_acc;
+  var = var_out;
+  min_ratio = mr;
+}
+
+// Finish one point in the lane that owns the v row (lane 0 of the quad for logdet): FP64 re-conditioning
+// below the pivot threshold, then the output (value, xi) or the logdet partial.
+template <typename T, int K, int D, bool LOGDET>
+__device__ __forceinline__ void quad_finish(const RefineParams<T>& p, bool gen, long long row, bool ok, T mean, T var,
+                                            T mr, double& acc_logdet) {
+  const long long r0 = row - p.n0;
+  double md = (double)mean, vd = (double)var;
+  if constexpr (sizeof(T) == 4) {
+    if (!(mr >= (T)p.tau)) {
+      int ids[K];
+      double vals[K];
+      for (int m = 0; m < p.k && m < K; ++m) {
+        int id = __ldg(p.nbrs + r0 * p.k + m);
+        ids[m] = (id < 0 || (long long)id >= p.n) ? 0 : id;
+        vals[m] = LOGDET ? 0.0 : (double)(gen ? ld_relaxed(p.values + ids[m]) : __ldg(p.values + ids[m]));
+      }
+      condition_point_f64<T, K>(p.points, D, row, ids, p.k, vals, !LOGDET, global_table_view<double>(p.tb),
+                                p.tb.desc->c0, &md, &vd);
+      atomicAdd(&p.status->fallback_count, 1u);
+    }
+  }
+  if (LOGDET) {
+    const double l = 0.5 * log(vd);
+    if (l != l) atomicOr(&p.status->nan_seen, 1u);
+    acc_logdet += l;
+    return;
+  }
+  const T sd = (T)sqrt(vd);
+  const T mu = (T)md;
+  if (gen) {
+    const T x = p.perm ? __ldg(p.xi + __ldg(p.perm + row)) : __ldg(p.xi + r0);
+    T out = canonical(fma(sd, x, mu));
+    if (!ok) {
+      out = canonical(out + (T)NAN);
+      atomicAdd(&p.status->timeouts, 1u);
+      report_error(p.status, GGP_ERR_TIMEOUT);
+    }
+    if (out != out) atomicOr(&p.status->nan_seen, 1u);
+    st_relaxed(p.values + row, out);
+    if (p.out_user) p.out_user[__ldg(p.perm + row)] = out;
+  } else {
+    const T out = canonical((__ldg(p.values + row) - mu) / sd);
+    if (out != out) atomicOr(&p.status->nan_seen, 1u);
+    if (p.out_user) p.out_user[__ldg(p.perm + row)] = out; else p.xi_out[r0] = out;
+  }
+}
+
+template <typename T, int K, int D, bool PAD, bool LOGDET>
+__global__ void __launch_bounds__(256) refine_quad2_kernel(RefineParams<T> p) {
+  constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
+  using SM = QuadSmem<K, D>;
+  extern __shared__ __align__(32) unsigned char smem[];
+  __shared__ double s_part[8];
+  const TableView<T> tab = stage_table<T>(p.tb, smem);
+  const int warp = threadIdx.x >> 5;
+  T* scratch = reinterpret_cast<T*>(smem + p.table_smem) + (size_t)warp * 8 * SM::kPerPoint;
+  const T c0 = (T)p.tb.desc->c0;
+  const int lane = threadIdx.x & 31;
+  const int g = lane & (kQuad - 1);
+  const int q = lane >> 2;
+  const int src0 = lane & ~(kQuad - 1);
+  T* crd = scratch + q * SM::kPerPoint;                      // (K+1) x kPointStride
+  T* tri = crd + (K + 1) * SM::kPointStride;                 // kPairs
+  const bool gen = !LOGDET && p.mode == kGenerate;
+  const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
+  const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
+  double acc_logdet = 0.0;
+  for (;;) {
+    const unsigned int t = warp_ticket(&p.status->ticket);
+    if (t >= total) break;
+    const int b = find_batch(p.chunk_prefix, p.n_batches, t);
+    long long bstart = (long long)__ldg(p.offsets + b);
+    bstart = bstart < p.n0 ? p.n0 : bstart;
+    long long end = __ldg(p.offsets + b + 1);
+    end = end > p.n ? p.n : end;
+    const int rpc = chunk_rows((long long)__ldg(p.offsets + b + 1) - (long long)__ldg(p.offsets + b));
+    const long long cbase = bstart + (long long)(t - (unsigned int)__ldg(p.chunk_prefix + b)) * rpc;
+    for (int sub = 0; sub < rpc; sub += 8) {
+      if (cbase + sub >= end) break;  // warp-uniform
+      const long long row = cbase + sub + q;
+      const bool active = row < end;
+      bool ok = true;
+      T P[NT][D];
+      T val[NT];
+      quad_load<T, K, D, PAD>(p, active, gen, may_wait, active ? row : bstart, bstart, g, P, val, ok);
+#pragma unroll
+      for (int tt = 0; tt < NT; ++tt) {
+        const int i = tt * kQuad + g;
+        if (i <= K) {
+#pragma unroll
+          for (int c = 0; c < D; ++c) crd[i * SM::kPointStride + c] = P[tt][c];
+        }
+      }
+      __syncwarp();
+      // phase 1: covariances of all pairs i > j, pair index p = i(i-1)/2 + j, dealt p = g, g+4, ...
+      {
+        int i = 1, j = g;
+        while (j >= i) { j -= i; ++i; }
+        const int kk = p.k;
+        for (int pp = g; pp < SM::kPairs; pp += kQuad) {
+          T a = T(0);
+          if (!(PAD && ((i < K && i >= kk) || j >= kk))) {
+            T pi[D], pj[D];
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+              pi[c] = crd[i * SM::kPointStride + c];
+              pj[c] = crd[j * SM::kPointStride + c];
+            }
+            a = tab(point_distance<T, D>(pi, pj));
+          }
+          tri[pp] = a;
+          j += kQuad;
+          while (j >= i && i <= K) { j -= i; ++i; }
+        }
+      }
+      __syncwarp();
+      T mean, var, mr;
+      quad_condition_tri<T, K, !LOGDET>(tri, val, g, src0, c0, mean, var, mr);
+      __syncwarp();  // the scratch is reused by the next sub-iteration
+      mr = quad_min(mr);
+      int okv = ok ? 1 : 0;  // quad-wide AND, both shuffles executed by every lane
+      okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
+      okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
+      const int g_out = LOGDET ? 0 : (K + 1) % kQuad;
+      if (active && g == g_out) quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, mr, acc_logdet);
+    }
+  }
+  if (LOGDET) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc_logdet += __shfl_xor_sync(0xffffffffu, acc_logdet, o);
+    if (lane == 0) s_part[threadIdx.x >> 5] = acc_logdet;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += s_part[w];
+      p.logdet_partials[blockIdx.x] = s;
+    }
+  }
+}
+
 }  // namespace ggp
