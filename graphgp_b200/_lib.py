@@ -81,6 +81,7 @@ _SIGS = {
     "ggp_refine_inv_f64": ([_P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _SZ, _P], _I),
     "ggp_refine_logdet_f32": ([_P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _D, _P, _SZ, _P], _I),
     "ggp_refine_logdet_f64": ([_P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _SZ, _P], _I),
+    "ggp_refine_logdet_f32_noalloc": ([_P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _D, _P], _I),
     "ggp_dense_f32": ([_I, _P, _I64, _I, _P, _P, _I, _P, _P, _P, _P, _SZ, _P], _I),
     "ggp_dense_f64": ([_I, _P, _I64, _I, _P, _P, _I, _P, _P, _P, _P, _SZ, _P], _I),
     "ggp_generate_f32": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _D, _U64, _P, _SZ, _P], _I),

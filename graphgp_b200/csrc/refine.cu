@@ -526,3 +526,77 @@ int ggp_generate_logdet_f64(const double* points, int64_t n, int d, int64_t n0, 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Log-determinant without a caller workspace.
+//
+// Some callers cannot allocate device memory for a workspace: a framework that reserves nearly all of the
+// GPU for its own memory pool (so a foreign cudaMalloc fails), a foreign-function handler that is given no
+// scratch allocator, or a latency-critical loop that must never enter an allocator. For them this entry
+// point runs the same refine_logdet computation with its scratch taken from a fixed array in device memory
+// that the library owns: kNoAllocScratchBytes (1 MiB) on every GPU that loads the library, held until the
+// process exits. That bounds the table to 4097 entries and the offsets array to 100,000 entries; larger
+// inputs are rejected with GGP_ERR_UNSUPPORTED before anything runs.
+//
+// The array's name is only meaningful to device code; host code needs its device address, which the first
+// call on each device looks up (cudaGetSymbolAddress, with that device current) and caches. Make that first
+// call on each device before any stream capture. Every call on a device shares the one array and leaves its
+// contents behind; each call clears what has to start at zero (the status block and the partial sums)
+// itself, but calls whose work overlaps on the GPU (different streams, or host threads) race on the array
+// and must be serialised by the caller.
+// ------------------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up once per device).
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return GGP_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      fprintf(stderr, "graphgp_b200: cudaGetSymbolAddress of the static scratch failed: %s\n",
+              cudaGetErrorString(e));
+      return GGP_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return GGP_OK;
+}
+
+}  // namespace
+
+extern "C" int ggp_refine_logdet_f32_noalloc(const float* points, int64_t n, int d, int64_t n0,
+                                             const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                                             const float* cov_bins, const float* cov_vals, int n_bins,
+                                             double* out_logdet, double tau, ggp_stream_t stream) {
+  Workspace need;
+  carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, n_bins < 2 ? 2 : n_bins, n_offsets < 1 ? 1 : n_offsets, 4,
+                  nullptr, 0, &need);
+  if (need.total > kNoAllocScratchBytes) {
+    fprintf(stderr,
+            "graphgp_b200: ggp_refine_logdet_f32_noalloc needs %zu bytes of scratch, more than its fixed %zu "
+            "(at most 4097 table entries and 100000 offsets); use ggp_refine_logdet_f32 with a workspace\n",
+            need.total, kNoAllocScratchBytes);
+    return GGP_ERR_UNSUPPORTED;
+  }
+  void* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  return refine_logdet_impl<float>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
+                                   out_logdet, tau, scratch, kNoAllocScratchBytes, GGP_STREAM(stream));
+}

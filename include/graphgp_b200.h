@@ -173,6 +173,19 @@ int ggp_refine_logdet_f64(const double* points, int64_t n, int d, int64_t n0, co
                           int n_bins, double* out_logdet, void* workspace, size_t workspace_bytes,
                           ggp_stream_t stream);
 
+/* ggp_refine_logdet_f32 for callers that cannot allocate device memory -- no counterpart in the reference.
+ * Frameworks that reserve nearly all of the GPU for their own memory pool, foreign-function handlers that
+ * are given no scratch allocator, and loops that must not enter an allocator can call this instead: it takes
+ * no workspace and uses a fixed 1 MiB array of device memory owned by the library (held on every GPU that
+ * loads it until exit), so inputs are limited to 4097 table entries and 100000 offsets (larger ones return
+ * GGP_ERR_UNSUPPORTED). The first call on each device looks up the array's address; make it before any
+ * stream capture. All calls on a device share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. *out_logdet is a device double. */
+int ggp_refine_logdet_f32_noalloc(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors,
+                                  int k, const int32_t* offsets, int n_offsets, const float* cov_bins,
+                                  const float* cov_vals, int n_bins, double* out_logdet, double tau,
+                                  ggp_stream_t stream);
+
 /* ---------------------------------------------------------------------------------------------- */
 /* Dense root in FP64 (reference graphgp/refine.py:59-76, 186-195, 243-248: jnp.linalg.cholesky,     */
 /* L @ xi, solve(L, v), slogdet(K)/2). Points / xi / values in T, factorisation and sums in FP64.  */
