@@ -2,7 +2,7 @@
 
 Every ``csrc/*.cu`` and ``csrc/inst/*.cu`` unit is compiled with nvcc in parallel (the register-resident
 kernel instantiations are split across units for that reason) and linked with ``-shared``. A unit is
-rebuilt when it, or any header under ``csrc/`` or ``include/``, is newer than its object file.
+rebuilt when it, or any header it includes (transitively), is newer than its object file.
 
 Usage: ``python -m graphgp_b200.build [--force] [--jobs N] [--verbose]``.
 """
@@ -11,6 +11,7 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -38,9 +39,19 @@ def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu")) + sorted((CSRC / "inst").glob("*.cu"))
 
 
-def _headers_mtime() -> float:
-    hs = list(CSRC.rglob("*.cuh")) + list((ROOT / "include").glob("*.h"))
-    return max((h.stat().st_mtime for h in hs), default=0.0)
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps_mtime(src: Path, seen=None) -> float:
+    """Newest modification time of `src` and every quoted header it includes, transitively."""
+    seen = set() if seen is None else seen
+    if src in seen or not src.exists():
+        return 0.0
+    seen.add(src)
+    t = src.stat().st_mtime
+    for inc in _INCLUDE.findall(src.read_text()):
+        t = max(t, _deps_mtime((src.parent / inc).resolve(), seen))
+    return t
 
 
 def _obj_for(src: Path) -> Path:
@@ -62,11 +73,10 @@ def _compile(src: Path, verbose: bool) -> tuple[Path, str]:
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     srcs = sources()
-    hdr = _headers_mtime()
     todo = []
     for s in srcs:
         o = _obj_for(s)
-        if force or not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, hdr):
+        if force or not o.exists() or o.stat().st_mtime < _deps_mtime(s.resolve()):
             todo.append(s)
     logs = []
     if todo:

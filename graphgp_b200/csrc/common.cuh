@@ -27,8 +27,9 @@ struct DeviceStatus {
   unsigned int fallback_count; // points re-conditioned in FP64 (pivot below threshold)
   unsigned int timeouts;       // bounded waits that ran out
   unsigned int ticket;         // work counter for persistent kernels
-  unsigned int ticket2;
-  unsigned int pad[58];        // keeps the struct at 256 bytes
+  unsigned int ticket2;        // second work counter (reverse sweep of the adjoint)
+  unsigned int done;           // chunks finished by the reverse sweep
+  unsigned int pad[57];        // keeps the struct at 256 bytes
 };
 static_assert(sizeof(DeviceStatus) == 256, "status block must be 256 bytes");
 

@@ -419,9 +419,3 @@ int ggp_build_graph_f64(const double* points, int64_t n, int d, int64_t n0, int 
 
 }  // extern "C"
 
-namespace ggp {
-size_t vjp_extra_bytes(long long n, long long n0, int k, int tbytes) {
-  (void)n; (void)n0; (void)k; (void)tbytes;
-  return 0;
-}
-}  // namespace ggp

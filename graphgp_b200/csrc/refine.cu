@@ -7,6 +7,7 @@
 #include "refine_generic.cuh"
 #include "workspace.cuh"
 #include "refine_launch.cuh"
+#include "vjp.cuh"
 
 namespace ggp {
 
@@ -523,6 +524,113 @@ int ggp_generate_logdet_f64(const double* points, int64_t n, int d, int64_t n0, 
                             ggp_stream_t stream) {
   return generate_logdet_impl<double>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
                                       out_logdet, 0.0, workspace, workspace_bytes, GGP_STREAM(stream));
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Adjoint of generate (vjp.cuh): forward recompute, reverse sweep, FP64 dense-root adjoint.
+// ------------------------------------------------------------------------------------------------
+namespace ggp {
+
+constexpr int kVjpMaxGrid = 1184;  // reverse-sweep blocks (rows of the bracket partials)
+constexpr int kRootHistGrid = 296;
+
+size_t vjp_extra_bytes(long long n, long long n0, int k, int nb, int tbytes) {
+  (void)k;
+  Carver c(nullptr);
+  c.take((size_t)tbytes * n);                                          // vbar
+  c.take(sizeof(double) * (size_t)(kVjpMaxGrid + kRootHistGrid) * nb);  // bracket partials
+  for (int b = 0; b < 3; ++b) c.take(sizeof(double) * (size_t)n0 * n0);  // L^T, Q -> X, X^T -> Kbar^T
+  return c.off;
+}
+
+template <typename T>
+int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
+                        const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* xi,
+                        const T* g_values, double g_logdet, T* out_grad_xi, double* out_grad_vals, double tau,
+                        void* wsp, size_t ws_bytes, cudaStream_t s) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !xi || !g_values || !out_grad_xi || !out_grad_vals) return GGP_ERR_INVALID;
+  if (k > kVjpMaxK || d > kVjpMaxD) return GGP_ERR_UNSUPPORTED;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_GENERATE_VJP, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  Carver c(ws.extra);
+  T* vbar = (T*)c.take(sizeof(T) * (size_t)n);
+  double* partials = (double*)c.take(sizeof(double) * (size_t)(kVjpMaxGrid + kRootHistGrid) * nb);
+  double* LT = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
+  double* X = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
+  double* XT = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  // forward recompute: values in graph order (workspace), dense factor L0 kept in ws.dense
+  T* vg = (T*)ws.values_graph;
+  (ggp::count_launch(), init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, nullptr, n0, n, offsets, n_offsets));
+  if ((rc = dense_root<T>(ws, points, n0, d, 0, xi, perm, vg, nullptr, nullptr, s))) return rc;
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
+  p.values = vg;
+  p.xi = perm ? xi : xi + n0;
+  p.perm = perm;
+  if ((rc = run_cond<T>(p, kGenerate, nb, s))) return rc;
+  // reverse sweep over the refined points
+  (ggp::count_launch(), gather_kernel<T><<<grid_for(n), 256, 0, s>>>(g_values, perm, vbar, n));
+  cudaMemsetAsync(partials, 0, sizeof(double) * (size_t)(kVjpMaxGrid + kRootHistGrid) * nb, s);
+  VjpParams<T> v{};
+  v.r = p;
+  v.r.table_smem = (int)((table_smem_bytes<T>(nb) + 255) / 256 * 256);
+  v.vbar = vbar;
+  v.grad_xi = out_grad_xi;
+  v.hist_partials = partials;
+  v.nb = nb;
+  v.g_logdet = g_logdet;
+  if (n > n0 && n_offsets > 1) {
+    const size_t smem = v.r.table_smem + sizeof(double) * (size_t)nb;
+    auto kern = vjp_refine_kernel<T>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int grid = persistent_grid(kern, 128, smem, kVjpMaxGrid);
+    (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(v));
+  }
+  // dense root: xibar0 = L^T vbar0, Kbar0 = L^-T Q L^-1
+  const double* L0 = ws.dense;
+  double* y = ws.dense_x;
+  (ggp::count_launch(), root_y_kernel<T><<<grid_for(n0 * 32), 256, 0, s>>>(L0, n0, vbar, xi, perm, y, out_grad_xi));
+  (ggp::count_launch(), transpose_kernel<<<grid_for(n0 * n0), 256, 0, s>>>(L0, n0, LT));
+  (ggp::count_launch(), root_q_kernel<T><<<grid_for(n0 * n0), 256, 0, s>>>(y, xi, perm, n0, g_logdet, X));
+  (ggp::count_launch(), row_solve_kernel<<<grid_for(n0 * 32), 256, 0, s>>>(X, LT, n0, 1));
+  (ggp::count_launch(), transpose_kernel<<<grid_for(n0 * n0), 256, 0, s>>>(X, n0, XT));
+  (ggp::count_launch(), row_solve_kernel<<<grid_for(n0 * 32), 256, 0, s>>>(XT, LT, n0, 0));
+  const size_t hsmem = sizeof(double) * (size_t)nb;
+  cudaFuncSetAttribute(root_hist_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  (ggp::count_launch(), root_hist_kernel<T><<<kRootHistGrid, 256, hsmem, s>>>(XT, points, n0, d, ws.table, nb,
+                                                                               partials + (size_t)kVjpMaxGrid * nb));
+  (ggp::count_launch(), reduce_columns_kernel<<<(nb + 255) / 256, 256, 0, s>>>(partials, kVjpMaxGrid + kRootHistGrid, nb,
+                                                                               out_grad_vals));
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace ggp
+
+extern "C" {
+
+int ggp_generate_vjp_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const float* cov_bins,
+                         const float* cov_vals, int n_bins, const float* xi, const float* g_values, double g_logdet,
+                         float* out_grad_xi, double* out_grad_vals, double tau, void* workspace,
+                         size_t workspace_bytes, ggp_stream_t stream) {
+  return generate_vjp_device<float>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
+                                    n_bins, xi, g_values, g_logdet, out_grad_xi, out_grad_vals, tau, workspace,
+                                    workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                         const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const double* cov_bins,
+                         const double* cov_vals, int n_bins, const double* xi, const double* g_values, double g_logdet,
+                         double* out_grad_xi, double* out_grad_vals, void* workspace, size_t workspace_bytes,
+                         ggp_stream_t stream) {
+  return generate_vjp_device<double>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
+                                     n_bins, xi, g_values, g_logdet, out_grad_xi, out_grad_vals, 0.0, workspace,
+                                     workspace_bytes, GGP_STREAM(stream));
 }
 
 }  // extern "C"

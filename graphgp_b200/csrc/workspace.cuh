@@ -34,7 +34,7 @@ struct Carver {
 
 // Extra bytes an op needs beyond the common regions (graph build scratch etc.); defined with the op.
 size_t graph_extra_bytes(int op, long long n, int d, long long n0, int k, int tbytes);
-size_t vjp_extra_bytes(long long n, long long n0, int k, int tbytes);
+size_t vjp_extra_bytes(long long n, long long n0, int k, int nb, int tbytes);
 
 inline int carve_workspace(int op, long long n, int d, long long n0, int k, int nb, int n_offsets, int tbytes,
                            void* base, size_t bytes, Workspace* ws) {
@@ -58,7 +58,7 @@ inline int carve_workspace(int op, long long n, int d, long long n0, int k, int 
   }
   size_t extra = 0;
   if (op >= GGP_OP_BUILD_TREE && op <= GGP_OP_ORDER_BY_DEPTH) extra = graph_extra_bytes(op, n, d, n0, k, tbytes);
-  if (op == GGP_OP_GENERATE_VJP) extra = vjp_extra_bytes(n, n0, k, tbytes);
+  if (op == GGP_OP_GENERATE_VJP) extra = vjp_extra_bytes(n, n0, k, nb > 1 ? nb : 2, tbytes);
   if (extra) {
     w.extra = c.take(extra);
     w.extra_bytes = extra;

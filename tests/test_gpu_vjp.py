@@ -1,0 +1,96 @@
+"""GPU adjoint of generate (ggp_generate_vjp_*) against the hand-written FP64 oracle adjoint (itself checked
+against finite differences in tests/test_oracle_adjoint.py) and against central finite differences of the GPU
+forward pass.
+
+Tolerances: FP64 kernels 1e-8 relative (norm-wise); FP32 kernels 1e-4 for the gradient with respect to xi and
+1e-3 for the gradient with respect to the table values (a sum of millions of FP32 terms per bracket).
+"""
+import numpy as np
+import pytest
+
+from oracle import adjoint as oa
+
+from conftest import rel_err
+from helpers import oracle_graph, matern32_table, rbf_table
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(x, dev, dtype=None):
+    import torch
+
+    t = torch.as_tensor(np.ascontiguousarray(x), device=dev)
+    return t if dtype is None else t.to(dtype)
+
+
+CASES = [(2000, 2, 100, 10, "rbf", 0.0), (2500, 3, 128, 16, "matern", 0.7), (1500, 2, 64, 20, "rbf", -1.3),
+         (1200, 3, 64, 7, "matern", 0.0)]
+
+
+def _table(name):
+    return rbf_table(scale=0.3) if name == "rbf" else matern32_table(cutoff=0.4)
+
+
+@pytest.mark.parametrize("n,d,n0,k,tab,gl", CASES)
+def test_vjp_f64_vs_oracle(cuda_device, n, d, n0, k, tab, gl):
+    from graphgp_b200 import graphgp_cuda as gc
+
+    pts, g = oracle_graph(n, d, n0, k)
+    bins, vals = _table(tab)
+    rng = np.random.default_rng(n + k)
+    xi, gv = rng.standard_normal(n), rng.standard_normal(n)
+    rx, rv = oa.generate_vjp(g, (bins, vals), xi, gv, gl)
+    gx, gvals = gc.generate_vjp(_t(g.points.astype(np.float64), cuda_device), _t(g.indices, cuda_device),
+                                _t(g.neighbors, cuda_device), g.offsets, _t(bins, cuda_device), _t(vals, cuda_device),
+                                _t(xi, cuda_device), _t(gv, cuda_device), gl)
+    st = gc.last_status()
+    assert st["error"] == 0 and st["timeouts"] == 0
+    assert rel_err(gx.cpu().numpy(), rx) < 1e-8
+    assert rel_err(gvals.cpu().numpy(), rv) < 1e-8
+
+
+@pytest.mark.parametrize("n,d,n0,k,tab,gl", CASES[:3])
+def test_vjp_f32_vs_oracle(cuda_device, n, d, n0, k, tab, gl):
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    pts, g = oracle_graph(n, d, n0, k)
+    bins, vals = _table(tab)
+    rng = np.random.default_rng(n + k + 1)
+    xi, gv = rng.standard_normal(n), rng.standard_normal(n)
+    rx, rv = oa.generate_vjp(g, (bins, vals), xi, gv, gl)
+    f32 = torch.float32
+    gx, gvals = gc.generate_vjp(_t(g.points, cuda_device), _t(g.indices, cuda_device), _t(g.neighbors, cuda_device),
+                                g.offsets, _t(bins, cuda_device, f32), _t(vals, cuda_device, f32),
+                                _t(xi, cuda_device, f32), _t(gv, cuda_device, f32), gl)
+    assert rel_err(gx.cpu().numpy(), rx) < 1e-4
+    assert rel_err(gvals.cpu().numpy(), rv) < 1e-3
+
+
+def test_vjp_finite_differences_on_gpu(cuda_device):
+    """<grad, direction> equals the central difference of the GPU forward (FP64) along random directions."""
+    from graphgp_b200 import graphgp_cuda as gc
+
+    n, d, n0, k = 3000, 2, 128, 12
+    pts, g = oracle_graph(n, d, n0, k)
+    bins, vals = matern32_table(cutoff=0.4)
+    rng = np.random.default_rng(5)
+    xi, gv, gl = rng.standard_normal(n), rng.standard_normal(n), 0.5
+    args = (_t(g.points.astype(np.float64), cuda_device), _t(g.indices, cuda_device), _t(g.neighbors, cuda_device),
+            g.offsets)
+    B = _t(bins, cuda_device)
+    gx, gvals = gc.generate_vjp(*args, B, _t(vals, cuda_device), _t(xi, cuda_device), _t(gv, cuda_device), gl)
+    gx, gvals = gx.cpu().numpy(), gvals.cpu().numpy()
+
+    def loss(x, vv):
+        v = gc.generate(*args, B, _t(vv, cuda_device), _t(x, cuda_device)).cpu().numpy()
+        ld = float(gc.generate_logdet(args[0], args[2], args[3], B, _t(vv, cuda_device)))
+        return float(np.dot(gv, v)) + gl * ld
+
+    h = 1e-6
+    for _ in range(4):
+        dx = rng.standard_normal(n)
+        dv = rng.standard_normal(len(vals)) * 1e-2
+        fd = (loss(xi + h * dx, vals + h * dv) - loss(xi - h * dx, vals - h * dv)) / (2 * h)
+        an = float(gx @ dx + gvals @ dv)
+        assert abs(fd - an) <= 1e-5 * max(1.0, abs(fd))
