@@ -272,9 +272,33 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
 
-    extra = {}
+    # generate + gradient: forward, residual against a fixed target, adjoint (w.r.t. xi and the table values)
+    Y = out + 0.01 * torch.randn(n, generator=torch.Generator(device=dev).manual_seed(5), device=dev)
+
+    def grad_step():
+        v = gc.generate(gp, gi, gn, OF, B, V, XI)
+        return gc.generate_vjp(gp, gi, gn, OF, B, V, XI, v - Y, 1.0)
+
+    for _ in range(2):
+        grad_step()
+    torch.cuda.synchronize()
+    gst = gc.last_status()
+    barrier(world)
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(args.steps):
+        grad_step()
+    e1.record()
+    torch.cuda.synchronize()
+    grad_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+
+    extra = {"generate_grad": {"value": n * world / (grad_ms * 1e-3), "unit": "points/s", "ms_per_step": grad_ms,
+                               "step": "generate, residual v - y, adjoint of 0.5|v - y|^2 + logdet w.r.t. xi and "
+                                       "the table values", "status_error": gst["error"] if gst else None}}
     if rank == 0 and not args.quick:
-        extra = comparisons(args, dev, gp, gi, gn, offs, OF, B, V, XI, pts, bins, vals, out, ms)
+        extra.update(comparisons(args, dev, gp, gi, gn, offs, OF, B, V, XI, pts, bins, vals, out, ms))
+    if rank == 0 and args.serving_requests > 0:
+        extra["serving"] = serving(dev, args.serving_requests)
 
     peaks = {}
     try:
@@ -318,6 +342,32 @@ def run_ours(args, world, rank, local):
         if not args.quick:
             line["cpu_baseline"] = cpu_baseline(gp, gn, offs, bins, vals)
         print(json.dumps(line), flush=True)
+
+
+def serving(dev, n_requests):
+    """The request stream (Poisson arrivals at 2000 req/s, uneven N, d, k, op mix 70/20/10) through the serving
+    engine: 16 slots (one CUDA stream each), 64 GiB admission budget, latency = completion - arrival."""
+    import torch
+
+    from graphgp_b200 import serving as sv
+
+    eng = sv.Engine(dev, slots=16, hbm_budget=64 << 30)
+    eng.run(sv.synthetic_stream(n_requests=48, seed=1, median_n=20000), realtime=False)  # warm-up
+    t = time.perf_counter()
+    reqs = sv.synthetic_stream(n_requests=n_requests, rate=2000.0, seed=0)
+    gen_s = time.perf_counter() - t
+    torch.cuda.synchronize()
+    res, summ = eng.run(reqs, realtime=True)
+    bad = sum(1 for r in res if r.status and r.status.get("error"))
+    pts = np.array([r.n for r in reqs])
+    summ.update(workload="4096 requests, Poisson 2000 req/s, N lognormal(median 30000, log-sd 1) clipped to "
+                         "[1e3, 1e6], d in {2,3}, k in {8,16,32}, n0 = max(k, min(256, N // 100)), RBF table per "
+                         "request (scale U(0.05,0.5), r=0 + 999 log bins on [1e-4, 10]); op mix 70/20/10"
+                if n_requests == 4096 else f"{n_requests} requests of the same distribution",
+                total_points=int(pts.sum()), requests_with_error=bad, host_generation_s=gen_s,
+                latency="completion - arrival, queueing included; includes graph build, H2D of points and "
+                        "payload, the operation and D2H of the result")
+    return summ
 
 
 def read_traffic(units):
@@ -460,6 +510,7 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override the number of points (testing)")
     ap.add_argument("--quick", action="store_true", help="skip the FP64 comparators and CPU baseline")
     ap.add_argument("--ref-sample", type=int, default=200000)
+    ap.add_argument("--serving-requests", type=int, default=4096, help="0 skips the serving stream")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()

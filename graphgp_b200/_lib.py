@@ -63,6 +63,8 @@ _SIGS = {
     "ggp_version": ([], C.c_char_p),
     "ggp_workspace_size": ([_I, _I64, _I, _I64, _I, _I, _I, _I], _SZ),
     "ggp_launch_count": ([], C.c_uint64),
+    "ggp_set_dataflow_width": ([C.c_double], None),
+    "ggp_get_dataflow_width": ([], C.c_double),
     "ggp_read_status": ([_P, C.POINTER(Status), _P], _I),
     "ggp_build_tree_f32": ([_P, _I64, _I, _P, _P, _P, _P, _SZ, _P], _I),
     "ggp_build_tree_f64": ([_P, _I64, _I, _P, _P, _P, _P, _SZ, _P], _I),

@@ -113,6 +113,9 @@ __device__ __forceinline__ unsigned int warp_ticket(unsigned int* counter) {
   return __shfl_sync(0xffffffffu, t, 0);
 }
 
+// Process-wide width of the dependency-ordered launches (ggp_set_dataflow_width); 0 = full persistent grid.
+double dataflow_width();
+
 // Occupancy-safe persistent grid size for a kernel.
 template <typename Kernel>
 inline int persistent_grid(Kernel k, int block, size_t smem, int max_blocks) {

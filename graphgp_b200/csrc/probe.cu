@@ -10,6 +10,9 @@ namespace ggp {
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+static std::atomic<double> g_dataflow_width{4.0};
+double dataflow_width() { return g_dataflow_width.load(std::memory_order_relaxed); }
+
 __global__ void wait_probe_kernel(const float* flag, DeviceStatus* st, unsigned long long timeout_ns) {
   float v;
   if (!wait_ready(flag, v, timeout_ns)) {
@@ -41,3 +44,9 @@ extern "C" int ggp_wait_probe(uint64_t timeout_ns, int* out_code, void* workspac
 }
 
 extern "C" uint64_t ggp_launch_count(void) { return ggp::g_launches.load(std::memory_order_relaxed); }
+
+extern "C" void ggp_set_dataflow_width(double warps_per_chunk) {
+  ggp::g_dataflow_width.store(warps_per_chunk > 0.0 ? warps_per_chunk : 0.0, std::memory_order_relaxed);
+}
+
+extern "C" double ggp_get_dataflow_width(void) { return ggp::dataflow_width(); }

@@ -192,7 +192,9 @@ template <typename T>
 int run_cond(RefineParams<T> p, int mode, int nb, cudaStream_t s) {
   p.mode = mode;
   if (p.n_batches < 1 || p.n == p.n0) return GGP_OK;
-  return cuda_status(dispatch<T>(p, kCond, nb, 0, s));
+  // generate waits batch on batch: cap its width (4 warps per block is the smaller block of the fast kernels)
+  const int cap = (mode == kGenerate) ? dataflow_blocks(p.n, p.n0, p.n_batches, 4) : 0;
+  return cuda_status(dispatch<T>(p, kCond, nb, cap, s));
 }
 
 template <typename T>
@@ -589,7 +591,8 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
     auto kern = vjp_refine_kernel<T>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e);
-    const int grid = persistent_grid(kern, 128, smem, kVjpMaxGrid);
+    const int cap = dataflow_blocks(n, n0, n_offsets - 1, 4);
+    const int grid = persistent_grid(kern, 128, smem, cap > 0 && cap < kVjpMaxGrid ? cap : kVjpMaxGrid);
     (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(v));
   }
   // dense root: xibar0 = L^T vbar0, Kbar0 = L^-T Q L^-1

@@ -1,6 +1,8 @@
 // Shared parameters and helpers of the refinement kernels (refine_quad.cuh, refine_generic.cuh).
 #pragma once
 
+#include <cmath>
+
 #include "condition.cuh"
 
 namespace ggp {
@@ -36,6 +38,19 @@ struct RefineParams {
 // Rows per work chunk of a batch: 8 for small batches (their latency is on the critical path of
 // generate), 32 for large ones (fewer tickets).
 __host__ __device__ __forceinline__ int chunk_rows(long long batch_size) { return batch_size < 16384 ? 8 : 32; }
+
+// Block cap for a dependency-ordered launch over rows [n0, n) in n_batches batches: dataflow_width() warps per
+// average chunk of a batch (at least 8 warps), as blocks of warps_per_block; 0 = no cap.
+inline int dataflow_blocks(long long n, long long n0, int n_batches, int warps_per_block) {
+  const double w = dataflow_width();
+  if (!(w > 0.0) || n_batches < 1 || n <= n0) return 0;
+  const double avg = double(n - n0) / n_batches;
+  const double chunks = std::ceil(avg / chunk_rows((long long)avg));
+  double warps = std::ceil(w * chunks);
+  if (warps < 8) warps = 8;
+  const double blocks = std::ceil(warps / warps_per_block);
+  return blocks > 1e9 ? 0 : (int)blocks;
+}
 
 // Batch that holds chunk t: largest b with chunk_prefix[b] <= t.
 __device__ __forceinline__ int find_batch(const int* __restrict__ prefix, int nb, unsigned int t) {

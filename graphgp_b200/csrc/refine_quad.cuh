@@ -1,19 +1,20 @@
 // Refinement with four lanes per point ("quad"): generate (dataflow across depth batches), inverse and
 // log-determinant, FP32 with FP64 re-conditioning of ill-conditioned points (or FP64 throughout).
 //
-// Per point, the rows of a left-looking Cholesky are [nbr_0 .. nbr_{k-1}, self, v]: the covariance of the
-// k + 1 points (built on the fly from the k(r) table) plus a "v" row holding the neighbour values, so the
-// factorisation leaves z = L11^-1 v in that row. Column k then yields var = std^2 = K[k,k] - l21.l21 and,
-// in the v row, -(l21 . z) / std = -mean / std (reference graphgp/refine.py:130-135, 278-285:
-// mean = (L11^-T l21) . v = l21 . z).
+// Per point, a left-looking Cholesky of the covariance of [nbr_0 .. nbr_{k-1}, self] (built from the k(r)
+// table) gives L11, l21 = L[k, 0..k) and var = std^2 = K[k,k] - l21.l21; back substitution L11^T w = l21 then
+// gives the regression weights, and mean = w . v[nbrs] (reference graphgp/refine.py:130-135, 278-285:
+// mean_vec = L11^-T l21). None of this reads a neighbour value except the final k-term dot product, so in
+// generate a point factors its neighbourhood as soon as its warp takes it and waits for its neighbours' values
+// only for that dot product: the dependency chain through the depth batches costs one value load and a short
+// reduction per batch rather than a whole factorisation.
 //
 // Rows are dealt round-robin to the four lanes of a quad (row i -> lane i % 4, slot i / 4). Column j is
-// owned by lane j % 4: it broadcasts the point of row j, the neighbour value v_j and the entries
-// L[j][0..j) by warp shuffles; every lane accumulates A[i][j] - sum_m L[i][m] L[j][m] for its rows i >= j
-// (the owner's own row j is the diagonal, so the pivot costs no extra pass), the owner broadcasts the
-// pivot and each lane scales its column entries by rsqrt(pivot). A quad therefore holds only about a
-// quarter of the triangle in registers, and a point's latency is about a quarter of a single thread's --
-// which is what bounds the dependency chain through the depth batches in generate.
+// owned by lane j % 4: it broadcasts the point of row j and the entries L[j][0..j) by warp shuffles; every
+// lane accumulates A[i][j] - sum_m L[i][m] L[j][m] for its rows i >= j (the owner's own row j is the
+// diagonal, so the pivot costs no extra pass), the owner broadcasts the pivot and each lane scales its column
+// entries by rsqrt(pivot), keeping that reciprocal in its diagonal slot for the back substitution. A quad
+// holds about a quarter of the triangle in registers.
 //
 // Work unit: a chunk of `rows_per_chunk` (a multiple of 8) consecutive rows of one depth batch, taken by
 // one warp as 8 points at a time. Chunks are numbered batch after batch and handed out by a global
@@ -27,21 +28,55 @@ namespace ggp {
 
 constexpr int kQuad = 4;
 
+// Register slots per lane for the K + 1 rows of one point.
+template <int K> struct QuadRows { static constexpr int NT = (K + 1 + kQuad - 1) / kQuad; };
+
 template <typename T> __device__ __forceinline__ T quad_min(T v) {
   v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 1));
   v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 2));
   return v;
 }
 
-// Factor one point spread over a quad. `g` = lane within the quad, `src0` = lane of the quad's g == 0.
-// P[t] / val[t]: point and value of this lane's row t*4+g (point rows only). Returns var in every lane and
-// `mean` in the lane owning the v row (WITH_V).
-template <typename T, int K, int D, bool PAD, bool WITH_V>
-__device__ __forceinline__ void quad_condition(const T (&P)[(K + 2 + kQuad - 1) / kQuad][D],
-                                               const T (&val)[(K + 2 + kQuad - 1) / kQuad], int g, int src0, int kk,
-                                               const TableView<T>& tab, T c0, T& mean, T& var, T& min_ratio) {
-  constexpr int R = WITH_V ? K + 2 : K + 1;  // rows
-  constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
+template <typename T> __device__ __forceinline__ T quad_sum(T v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  return v;
+}
+
+// Back substitution L11^T w = l21 over the quad. L[t][m] is entry m of row i = t*4 + g of the factor, with
+// 1 / L[i][i] in the diagonal slot; row K holds l21. Each w_m (m = K-1 .. 0) is l21_m minus the quad sum of
+// the terms L[i][m] w_i of rows i > m, times the reciprocal pivot of row m; lane g keeps w_i of its own rows
+// i = t*4 + g < K in wmine[t] (0 for the self row and for padding rows).
+template <typename T, int K>
+__device__ __forceinline__ void quad_backsub(const T (&L)[QuadRows<K>::NT][K + 1], int g, int src0,
+                                             T (&wmine)[QuadRows<K>::NT]) {
+  constexpr int NT = QuadRows<K>::NT;
+  const int srcK = src0 + K % kQuad;
+#pragma unroll
+  for (int t = 0; t < NT; ++t) wmine[t] = T(0);
+#pragma unroll
+  for (int m = K - 1; m >= 0; --m) {
+    const T l = __shfl_sync(0xffffffffu, L[K / kQuad][m], srcK);
+    T part = T(0);
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+      if (t * kQuad + kQuad - 1 > m) part = fma(L[t][m], wmine[t], part);
+    part = quad_sum(part);
+    const T wm = (l - part) * L[m / kQuad][m];  // the reciprocal pivot is in the owner lane of row m
+    if (g == m % kQuad) wmine[m / kQuad] = wm;
+  }
+}
+
+// Factor one point spread over a quad, evaluating covariances inside the factorisation. `g` = lane within the
+// quad, `src0` = lane of the quad's g == 0. P[t]: point of this lane's row t*4+g (row K = the point itself).
+// Returns the weights of this lane's rows, var and the smallest pivot ratio (pivot / prior variance) in every
+// lane.
+template <typename T, int K, int D, bool PAD>
+__device__ __forceinline__ void quad_factor(const T (&P)[QuadRows<K>::NT][D], int g, int src0, int kk,
+                                            const TableView<T>& tab, T c0, T (&wmine)[QuadRows<K>::NT], T& var,
+                                            T& min_ratio) {
+  constexpr int R = K + 1;  // rows
+  constexpr int NT = QuadRows<K>::NT;
   T L[NT][K + 1];
 #pragma unroll
   for (int t = 0; t < NT; ++t)
@@ -49,19 +84,15 @@ __device__ __forceinline__ void quad_condition(const T (&P)[(K + 2 + kQuad - 1) 
     for (int m = 0; m <= K; ++m) L[t][m] = T(0);
   T mr = T(1);
   const T inv_c0 = T(1) / c0;
-  T mean_acc = T(0);
   T var_out = T(0);
 #pragma unroll
   for (int j = 0; j <= K; ++j) {
     const int o = j % kQuad;
     const int tj = j / kQuad;
     const int src = src0 + o;
-    // broadcast the point (and value) of row j
     T pj[D];
 #pragma unroll
     for (int c = 0; c < D; ++c) pj[c] = __shfl_sync(0xffffffffu, P[tj][c], src);
-    T vj = T(0);
-    if (WITH_V && j < K) vj = __shfl_sync(0xffffffffu, val[tj], src);
     const bool jdummy = PAD && j < K && j >= kk;
     // initial entries A[i][j] for my rows i >= j
     T acc[NT];
@@ -72,12 +103,8 @@ __device__ __forceinline__ void quad_condition(const T (&P)[(K + 2 + kQuad - 1) 
       if (t * kQuad + kQuad - 1 < j) { acc[t] = a; continue; }  // slot entirely above column j
       if (i == j) {
         a = c0;
-      } else if (i > j && i < R) {
-        if (WITH_V && i == K + 1) {
-          a = vj;  // v row: neighbour value (0 for the self column and dummies)
-        } else if (!(jdummy || (PAD && i < K && i >= kk))) {
-          a = tab(point_distance<T, D>(P[t], pj));
-        }
+      } else if (i > j && i < R && !(jdummy || (PAD && i < K && i >= kk))) {
+        a = tab(point_distance<T, D>(P[t], pj));
       }
       acc[t] = a;
     }
@@ -97,25 +124,24 @@ __device__ __forceinline__ void quad_condition(const T (&P)[(K + 2 + kQuad - 1) 
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       const int i = t * kQuad + g;
-      if (WITH_V && j == K && i == K + 1) mean_acc = -acc[t];  // v row at the self column: -(l21 . z)
-      if (t * kQuad + kQuad - 1 >= j) L[t][j] = (i > j && i < R) ? acc[t] * r : L[t][j];
+      if (t * kQuad + kQuad - 1 >= j) L[t][j] = (i > j && i < R) ? acc[t] * r : (i == j ? r : L[t][j]);
     }
   }
-  mean = mean_acc;
+  quad_backsub<T, K>(L, g, src0, wmine);
   var = var_out;
   min_ratio = mr;
 }
 
+// Neighbour ids and coordinates of this lane's rows (row K = the point itself); dummies / inactive rows get
+// id -1 and coordinates 0.
 template <typename T, int K, int D, bool PAD>
-__device__ __forceinline__ void quad_load(const RefineParams<T>& p, bool active, bool gen, bool may_wait,
-                                          long long row, long long bstart, int g,
-                                          T (&P)[(K + 2 + kQuad - 1) / kQuad][D], T (&val)[(K + 2 + kQuad - 1) / kQuad],
-                                          bool& ok) {
-  constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
+__device__ __forceinline__ void quad_load_coords(const RefineParams<T>& p, bool active, bool gen, long long row,
+                                                 long long bstart, int g, int (&ids)[QuadRows<K>::NT],
+                                                 T (&P)[QuadRows<K>::NT][D], bool& ok) {
+  constexpr int NT = QuadRows<K>::NT;
   const int kk = p.k;
   const long long r0 = row - p.n0;
   const long long lim = gen ? bstart : p.n;
-  int ids[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     const int i = t * kQuad + g;
@@ -130,23 +156,30 @@ __device__ __forceinline__ void quad_load(const RefineParams<T>& p, bool active,
     }
     ids[t] = id;
   }
-  // coordinates: neighbour rows, the self row (i == K); dummies / inactive stay at 0
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     const int i = t * kQuad + g;
 #pragma unroll
     for (int c = 0; c < D; ++c) P[t][c] = T(0);
-    val[t] = T(0);
     long long pid = -1;
     if (i < K && ids[t] >= 0) pid = ids[t];
     else if (i == K && active) pid = row;
     if (pid >= 0) load_point<T, D>(p.points, pid, P[t]);
   }
-  if (!p.values) return;
-  // neighbour values: issue all loads, then wait only where still pending
+}
+
+// mean = w . v[nbrs] over the quad: this lane loads the values of its rows (in generate waiting, bounded, on
+// those still pending), multiplies by its weights and the quad sums the four shares (every lane gets it).
+template <typename T, int K>
+__device__ __forceinline__ T quad_mean(const RefineParams<T>& p, bool gen, bool may_wait,
+                                       const int (&ids)[QuadRows<K>::NT], int g, const T (&wmine)[QuadRows<K>::NT],
+                                       bool& ok) {
+  constexpr int NT = QuadRows<K>::NT;
+  T val[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     const int i = t * kQuad + g;
+    val[t] = T(0);
     if (i < K && ids[t] >= 0) val[t] = gen ? ld_relaxed(p.values + ids[t]) : __ldg(p.values + ids[t]);
   }
   if (gen) {
@@ -165,12 +198,78 @@ __device__ __forceinline__ void quad_load(const RefineParams<T>& p, bool active,
       }
     }
   }
+  T part = T(0);
+#pragma unroll
+  for (int t = 0; t < NT; ++t) part = fma(wmine[t], val[t], part);
+  return quad_sum(part);
+}
+
+// FP64 weights and variance of a point whose FP32 pivot ratio fell below tau (computed before any wait).
+template <typename T, int K, int D>
+__device__ __forceinline__ void quad_refactor_f64(const RefineParams<T>& p, long long row, double (&w64)[K],
+                                                  double& vd64) {
+  const long long r0 = row - p.n0;
+  int ids[K];
+  for (int m = 0; m < p.k && m < K; ++m) {
+    const int id = __ldg(p.nbrs + r0 * p.k + m);
+    ids[m] = (id < 0 || (long long)id >= p.n) ? 0 : id;
+  }
+  condition_weights_f64<T, K>(p.points, D, row, ids, p.k, global_table_view<double>(p.tb), p.tb.desc->c0, w64, &vd64);
+}
+
+// Finish one point in lane 0 of its quad: the FP64 mean of a re-conditioned point, then the output (value,
+// xi) or the logdet partial.
+template <typename T, int K, int D, bool LOGDET>
+__device__ __forceinline__ void quad_finish(const RefineParams<T>& p, bool gen, long long row, bool ok, T mean, T var,
+                                            bool fb, const double (&w64)[K], double vd64, double& acc_logdet) {
+  const long long r0 = row - p.n0;
+  double md = (double)mean, vd = (double)var;
+  if constexpr (sizeof(T) == 4) {
+    if (fb) {
+      vd = vd64;
+      if (!LOGDET) {
+        double mu = 0.0;
+        for (int m = 0; m < p.k && m < K; ++m) {
+          int id = __ldg(p.nbrs + r0 * p.k + m);
+          id = (id < 0 || (long long)id >= p.n) ? 0 : id;
+          T v = gen ? ld_relaxed(p.values + id) : __ldg(p.values + id);  // ready: the quad waited for it
+          mu = fma(w64[m], (double)v, mu);
+        }
+        md = mu;
+      }
+      atomicAdd(&p.status->fallback_count, 1u);
+    }
+  }
+  if (LOGDET) {
+    const double l = 0.5 * log(vd);
+    if (l != l) atomicOr(&p.status->nan_seen, 1u);
+    acc_logdet += l;
+    return;
+  }
+  const T sd = (T)sqrt(vd);
+  const T mu = (T)md;
+  if (gen) {
+    const T x = p.perm ? __ldg(p.xi + __ldg(p.perm + row)) : __ldg(p.xi + r0);
+    T out = canonical(fma(sd, x, mu));
+    if (!ok) {
+      out = canonical(out + (T)NAN);
+      atomicAdd(&p.status->timeouts, 1u);
+      report_error(p.status, GGP_ERR_TIMEOUT);
+    }
+    if (out != out) atomicOr(&p.status->nan_seen, 1u);
+    st_relaxed(p.values + row, out);
+    if (p.out_user) p.out_user[__ldg(p.perm + row)] = out;
+  } else {
+    const T out = canonical((__ldg(p.values + row) - mu) / sd);
+    if (out != out) atomicOr(&p.status->nan_seen, 1u);
+    if (p.out_user) p.out_user[__ldg(p.perm + row)] = out; else p.xi_out[r0] = out;
+  }
 }
 
 // Generate (mode kGenerate) / inverse (kInverse) / log-determinant (LOGDET).
 template <typename T, int K, int D, bool PAD, bool LOGDET>
 __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
-  constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
+  constexpr int NT = QuadRows<K>::NT;
   extern __shared__ __align__(32) unsigned char smem[];
   __shared__ double s_part[4];
   const TableView<T> tab = stage_table<T>(p.tb, smem);
@@ -198,60 +297,23 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
       const long long row = cbase + sub + q;
       const bool active = row < end;
       bool ok = true;
+      int ids[NT];
       T P[NT][D];
-      T val[NT];
-      quad_load<T, K, D, PAD>(p, active, gen, may_wait, active ? row : bstart, bstart, g, P, val, ok);
-      T mean, var, mr;
-      quad_condition<T, K, D, PAD, !LOGDET>(P, val, g, src0, p.k, tab, c0, mean, var, mr);
+      quad_load_coords<T, K, D, PAD>(p, active, gen, active ? row : bstart, bstart, g, ids, P, ok);
+      T wmine[NT], var, mr;
+      quad_factor<T, K, D, PAD>(P, g, src0, p.k, tab, c0, wmine, var, mr);
       mr = quad_min(mr);
+      const bool fb = sizeof(T) == 4 && active && !(mr >= (T)p.tau);  // quad-uniform
+      double w64[K];
+      double vd64 = 0.0;
+      if (fb && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
+      T mean = T(0);
+      if (!LOGDET) mean = quad_mean<T, K>(p, gen, may_wait, ids, g, wmine, ok);
       // quad-wide AND; every lane executes both shuffles (no short-circuit around a warp intrinsic)
       int okv = ok ? 1 : 0;
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
-      ok = okv != 0;
-      // the lane that owns the v row (or lane 0 of the quad for logdet) finishes the point
-      const int g_out = LOGDET ? 0 : (K + 1) % kQuad;
-      if (!active || g != g_out) continue;
-      const long long r0 = row - p.n0;
-      double md = (double)mean, vd = (double)var;
-      if constexpr (sizeof(T) == 4) {
-        if (!(mr >= (T)p.tau)) {
-          int ids[K];
-          double vals[K];
-          for (int m = 0; m < p.k && m < K; ++m) {
-            int id = __ldg(p.nbrs + r0 * p.k + m);
-            ids[m] = (id < 0 || (long long)id >= p.n) ? 0 : id;
-            vals[m] = LOGDET ? 0.0 : (double)(gen ? ld_relaxed(p.values + ids[m]) : __ldg(p.values + ids[m]));
-          }
-          condition_point_f64<T, K>(p.points, D, row, ids, p.k, vals, !LOGDET, global_table_view<double>(p.tb),
-                                    p.tb.desc->c0, &md, &vd);
-          atomicAdd(&p.status->fallback_count, 1u);
-        }
-      }
-      if (LOGDET) {
-        const double l = 0.5 * log(vd);
-        if (l != l) atomicOr(&p.status->nan_seen, 1u);
-        acc_logdet += l;
-        continue;
-      }
-      const T sd = (T)sqrt(vd);
-      const T mu = (T)md;
-      if (gen) {
-        const T x = p.perm ? __ldg(p.xi + __ldg(p.perm + row)) : __ldg(p.xi + r0);
-        T out = canonical(fma(sd, x, mu));
-        if (!ok) {
-          out = canonical(out + (T)NAN);
-          atomicAdd(&p.status->timeouts, 1u);
-          report_error(p.status, GGP_ERR_TIMEOUT);
-        }
-        if (out != out) atomicOr(&p.status->nan_seen, 1u);
-        st_relaxed(p.values + row, out);
-        if (p.out_user) p.out_user[__ldg(p.perm + row)] = out;
-      } else {
-        const T out = canonical((__ldg(p.values + row) - mu) / sd);
-        if (out != out) atomicOr(&p.status->nan_seen, 1u);
-        if (p.out_user) p.out_user[__ldg(p.perm + row)] = out; else p.xi_out[r0] = out;
-      }
+      if (active && g == 0) quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
     }
   }
   if (LOGDET) {
@@ -282,11 +344,12 @@ template <int K, int D> struct QuadSmem {
   static constexpr int kPerPoint = (K + 1) * kPointStride + kPairs + 1;  // +1 staggers banks
 };
 
-template <typename T, int K, bool WITH_V>
-__device__ __forceinline__ void quad_condition_tri(const T* __restrict__ tri, const T (&val)[(K + 2 + kQuad - 1) / kQuad],
-                                                   int g, int src0, T c0, T& mean, T& var, T& min_ratio) {
-  constexpr int R = WITH_V ? K + 2 : K + 1;
-  constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
+// quad_factor with the off-diagonal covariances read from `tri` (pair (i, j), i > j, at i(i-1)/2 + j).
+template <typename T, int K>
+__device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g, int src0, T c0,
+                                                T (&wmine)[QuadRows<K>::NT], T& var, T& min_ratio) {
+  constexpr int R = K + 1;
+  constexpr int NT = QuadRows<K>::NT;
   T L[NT][K + 1];
 #pragma unroll
   for (int t = 0; t < NT; ++t)
@@ -294,15 +357,12 @@ __device__ __forceinline__ void quad_condition_tri(const T* __restrict__ tri, co
     for (int m = 0; m <= K; ++m) L[t][m] = T(0);
   T mr = T(1);
   const T inv_c0 = T(1) / c0;
-  T mean_acc = T(0);
   T var_out = T(0);
 #pragma unroll
   for (int j = 0; j <= K; ++j) {
     const int o = j % kQuad;
     const int tj = j / kQuad;
     const int src = src0 + o;
-    T vj = T(0);
-    if (WITH_V && j < K) vj = __shfl_sync(0xffffffffu, val[tj], src);
     T acc[NT];
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
@@ -311,7 +371,6 @@ __device__ __forceinline__ void quad_condition_tri(const T* __restrict__ tri, co
       if (t * kQuad + kQuad - 1 >= j) {
         if (i == j) a = c0;
         else if (i > j && i <= K) a = tri[i * (i - 1) / 2 + j];
-        else if (WITH_V && i == K + 1) a = vj;
       }
       acc[t] = a;
     }
@@ -329,65 +388,17 @@ __device__ __forceinline__ void quad_condition_tri(const T* __restrict__ tri, co
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       const int i = t * kQuad + g;
-      if (WITH_V && j == K && i == K + 1) mean_acc = -acc[t];
-      if (t * kQuad + kQuad - 1 >= j) L[t][j] = (i > j && i < R) ? acc[t] * r : L[t][j];
+      if (t * kQuad + kQuad - 1 >= j) L[t][j] = (i > j && i < R) ? acc[t] * r : (i == j ? r : L[t][j]);
     }
   }
-  mean = mean_acc;
+  quad_backsub<T, K>(L, g, src0, wmine);
   var = var_out;
   min_ratio = mr;
 }
 
-// Finish one point in the lane that owns the v row (lane 0 of the quad for logdet): FP64 re-conditioning
-// below the pivot threshold, then the output (value, xi) or the logdet partial.
-template <typename T, int K, int D, bool LOGDET>
-__device__ __forceinline__ void quad_finish(const RefineParams<T>& p, bool gen, long long row, bool ok, T mean, T var,
-                                            T mr, double& acc_logdet) {
-  const long long r0 = row - p.n0;
-  double md = (double)mean, vd = (double)var;
-  if constexpr (sizeof(T) == 4) {
-    if (!(mr >= (T)p.tau)) {
-      int ids[K];
-      double vals[K];
-      for (int m = 0; m < p.k && m < K; ++m) {
-        int id = __ldg(p.nbrs + r0 * p.k + m);
-        ids[m] = (id < 0 || (long long)id >= p.n) ? 0 : id;
-        vals[m] = LOGDET ? 0.0 : (double)(gen ? ld_relaxed(p.values + ids[m]) : __ldg(p.values + ids[m]));
-      }
-      condition_point_f64<T, K>(p.points, D, row, ids, p.k, vals, !LOGDET, global_table_view<double>(p.tb),
-                                p.tb.desc->c0, &md, &vd);
-      atomicAdd(&p.status->fallback_count, 1u);
-    }
-  }
-  if (LOGDET) {
-    const double l = 0.5 * log(vd);
-    if (l != l) atomicOr(&p.status->nan_seen, 1u);
-    acc_logdet += l;
-    return;
-  }
-  const T sd = (T)sqrt(vd);
-  const T mu = (T)md;
-  if (gen) {
-    const T x = p.perm ? __ldg(p.xi + __ldg(p.perm + row)) : __ldg(p.xi + r0);
-    T out = canonical(fma(sd, x, mu));
-    if (!ok) {
-      out = canonical(out + (T)NAN);
-      atomicAdd(&p.status->timeouts, 1u);
-      report_error(p.status, GGP_ERR_TIMEOUT);
-    }
-    if (out != out) atomicOr(&p.status->nan_seen, 1u);
-    st_relaxed(p.values + row, out);
-    if (p.out_user) p.out_user[__ldg(p.perm + row)] = out;
-  } else {
-    const T out = canonical((__ldg(p.values + row) - mu) / sd);
-    if (out != out) atomicOr(&p.status->nan_seen, 1u);
-    if (p.out_user) p.out_user[__ldg(p.perm + row)] = out; else p.xi_out[r0] = out;
-  }
-}
-
 template <typename T, int K, int D, bool PAD, bool LOGDET>
 __global__ void __launch_bounds__(256) refine_quad2_kernel(RefineParams<T> p) {
-  constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
+  constexpr int NT = QuadRows<K>::NT;
   using SM = QuadSmem<K, D>;
   extern __shared__ __align__(32) unsigned char smem[];
   __shared__ double s_part[8];
@@ -420,9 +431,9 @@ __global__ void __launch_bounds__(256) refine_quad2_kernel(RefineParams<T> p) {
       const long long row = cbase + sub + q;
       const bool active = row < end;
       bool ok = true;
+      int ids[NT];
       T P[NT][D];
-      T val[NT];
-      quad_load<T, K, D, PAD>(p, active, gen, may_wait, active ? row : bstart, bstart, g, P, val, ok);
+      quad_load_coords<T, K, D, PAD>(p, active, gen, active ? row : bstart, bstart, g, ids, P, ok);
 #pragma unroll
       for (int tt = 0; tt < NT; ++tt) {
         const int i = tt * kQuad + g;
@@ -454,15 +465,20 @@ __global__ void __launch_bounds__(256) refine_quad2_kernel(RefineParams<T> p) {
         }
       }
       __syncwarp();
-      T mean, var, mr;
-      quad_condition_tri<T, K, !LOGDET>(tri, val, g, src0, c0, mean, var, mr);
+      T wmine[NT], var, mr;
+      quad_factor_tri<T, K>(tri, g, src0, c0, wmine, var, mr);
       __syncwarp();  // the scratch is reused by the next sub-iteration
       mr = quad_min(mr);
+      const bool fb = sizeof(T) == 4 && active && !(mr >= (T)p.tau);  // quad-uniform
+      double w64[K];
+      double vd64 = 0.0;
+      if (fb && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
+      T mean = T(0);
+      if (!LOGDET) mean = quad_mean<T, K>(p, gen, may_wait, ids, g, wmine, ok);
       int okv = ok ? 1 : 0;  // quad-wide AND, both shuffles executed by every lane
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
-      const int g_out = LOGDET ? 0 : (K + 1) % kQuad;
-      if (active && g == g_out) quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, mr, acc_logdet);
+      if (active && g == 0) quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
     }
   }
   if (LOGDET) {

@@ -74,6 +74,14 @@ size_t ggp_workspace_size(int op, int64_t n, int d, int64_t n0, int k, int n_bin
  * the reference). */
 uint64_t ggp_launch_count(void);
 
+/* Width of the dependency-ordered (generate and adjoint) launches, in warps per average chunk of a batch
+ * (a chunk is the 8 or 32 consecutive rows one warp takes at a time). Those launches keep their warps resident
+ * while later batches wait for earlier ones; a width of about the largest batch's chunk count keeps a small
+ * graph's launch from holding every SM, so that work on other streams runs beside it. 0 = one full persistent
+ * grid (every SM at full occupancy). Default 4. Process-wide; no counterpart in the reference. */
+void ggp_set_dataflow_width(double warps_per_chunk);
+double ggp_get_dataflow_width(void);
+
 /* Copy the status block of a workspace to the host (synchronises `stream`). */
 int ggp_read_status(const void* workspace, ggp_status_t* out, ggp_stream_t stream);
 
