@@ -8,6 +8,7 @@
 #include "workspace.cuh"
 #include "refine_launch.cuh"
 #include "vjp.cuh"
+#include "vjp_quad.cuh"
 
 namespace ggp {
 
@@ -547,6 +548,14 @@ size_t vjp_extra_bytes(long long n, long long n0, int k, int nb, int tbytes) {
   return c.off;
 }
 
+template <typename T, int D>
+cudaError_t vjp_quad_dispatch_k(const VjpParams<T>& v, int k, int max_blocks, cudaStream_t s) {
+  if (k <= 8) return launch_vjp_quad<T, 8, D, true>(v, max_blocks, s);
+  if (k <= 10) return launch_vjp_quad<T, 10, D, true>(v, max_blocks, s);
+  if (k <= 16) return launch_vjp_quad<T, 16, D, true>(v, max_blocks, s);
+  return launch_vjp_quad<T, 20, D, true>(v, max_blocks, s);
+}
+
 template <typename T>
 int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                         const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* xi,
@@ -586,7 +595,13 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
   v.hist_partials = partials;
   v.nb = nb;
   v.g_logdet = g_logdet;
-  if (n > n0 && n_offsets > 1) {
+  bool swept = false;
+  if (n > n0 && n_offsets > 1 && k <= 20 && (d == 2 || d == 3)) {
+    cudaError_t e = d == 2 ? vjp_quad_dispatch_k<T, 2>(v, k, kVjpMaxGrid, s) : vjp_quad_dispatch_k<T, 3>(v, k, kVjpMaxGrid, s);
+    if (e == cudaSuccess) swept = true;
+    else if (e != cudaErrorInvalidConfiguration) return cuda_status(e);
+  }
+  if (!swept && n > n0 && n_offsets > 1) {
     const size_t smem = v.r.table_smem + sizeof(double) * (size_t)nb;
     auto kern = vjp_refine_kernel<T>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

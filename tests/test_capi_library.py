@@ -12,7 +12,7 @@ HEADER = ROOT / "include" / "graphgp_b200.h"
 
 def declared_symbols():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|size_t|uint64_t|const char\*)\s+(ggp_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|size_t|uint64_t|void|double|const char\*)\s+(ggp_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_entry_points():
