@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
       }
       __syncwarp();
       const T vb = active ? ld_relaxed(v.vbar + row) : T(0);
-      const long long uo = p.perm ? (long long)__ldg(p.perm + row) : row;
+      // rows past the batch end (inactive quads) may lie past n: read nothing for them
+      const long long uo = !active ? 0 : (p.perm ? (long long)__ldg(p.perm + row) : row);
       if (active && g == 0) v.grad_xi[uo] = canonical(sig * vb);
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
