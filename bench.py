@@ -299,6 +299,8 @@ def run_ours(args, world, rank, local):
         extra.update(comparisons(args, dev, gp, gi, gn, offs, OF, B, V, XI, pts, bins, vals, out, ms))
     if rank == 0 and args.serving_requests > 0:
         extra["serving"] = serving(dev, args.serving_requests)
+    if rank == 0 and args.fd_directions > 0:
+        extra["differentiation"] = differentiation(dev, n_dirs=args.fd_directions)
 
     peaks = {}
     try:
@@ -346,6 +348,98 @@ def run_ours(args, world, rank, local):
         if not args.quick:
             line["cpu_baseline"] = cpu_baseline(gp, gn, offs, bins, vals)
         print(json.dumps(line), flush=True)
+
+
+def differentiation(dev, n_dirs=64, steps=5, warmup=3, n=4194304):
+    """Generate + gradient on the differentiation workload: N = 4,194,304 points uniform in [0, 1]^2 (float32),
+    n0 = 256, k = 20, RBF scale 0.1 with r = 0 + 1,000 log bins on [1e-5, 1.5] (1,001 values), jitter 1e-4;
+    y = generate(xi*) + 0.01 N(0, 1); loss 0.5 |generate(xi) - y|^2 + logdet. Times the FP32 step (forward,
+    residual, adjoint w.r.t. xi and the table values) and checks <grad, u> against central differences of the
+    FP64 forward along n_dirs random directions: half move xi only (u standard normal, unit norm; the loss is
+    quadratic in xi, so differences with step 1e-3 are exact up to rounding), half move the table only
+    (u = 1e-3 vals * N(0, 1), a relative perturbation that keeps every joint covariance positive definite under
+    the jitter); there the loss is far from quadratic, so the differences are taken with steps 1e-3 and 1e-5."""
+    import torch
+
+    from graphgp_b200 import extras
+    from graphgp_b200 import graphgp_cuda as gc
+
+    rng = np.random.default_rng(2024)
+    pts = rng.uniform(0.0, 1.0, (n, 2)).astype(np.float32)
+    bins, vals = extras.rbf_kernel(variance=1.0, scale=0.1, r_min=1e-5, r_max=1.5, n_bins=1001, jitter=1e-4)
+    P = torch.as_tensor(pts, device=dev)
+    gp, gi, gn, _, offs = gc.build_graph(P, n0=256, k=20, return_offsets=True)
+    OF = torch.as_tensor(offs, dtype=torch.int32, device=dev)
+    B = torch.as_tensor(bins, dtype=torch.float32, device=dev)
+    V = torch.as_tensor(vals, dtype=torch.float32, device=dev)
+    xs = torch.as_tensor(rng.standard_normal(n).astype(np.float32), device=dev)
+    y = gc.generate(gp, gi, gn, OF, B, V, xs) + 0.01 * torch.as_tensor(rng.standard_normal(n).astype(np.float32),
+                                                                        device=dev)
+    xi = torch.as_tensor(rng.standard_normal(n).astype(np.float32), device=dev)
+
+    def step():
+        v = gc.generate(gp, gi, gn, OF, B, V, xi)
+        return gc.generate_vjp(gp, gi, gn, OF, B, V, xi, v - y, 1.0)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        gx, gv = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = gc.last_status()
+
+    # FP64 forward for the differences, and the FP64 adjoint beside the FP32 one
+    P64, B64, V64 = gp.double(), B.double(), torch.as_tensor(vals, dtype=torch.float64, device=dev)
+    y64, xi64 = y.double(), xi.double()
+
+    def loss64(x, vv):
+        v = gc.generate(P64, gi, gn, OF, B64, vv, x)
+        return 0.5 * float(torch.sum((v - y64) ** 2)) + float(gc.generate_logdet(P64, gn, OF, B64, vv))
+
+    v64 = gc.generate(P64, gi, gn, OF, B64, V64, xi64)
+    gx64, gv64 = gc.generate_vjp(P64, gi, gn, OF, B64, V64, xi64, v64 - y64, 1.0)
+    gx32, gv32 = gx.double(), gv.double()
+    h = 1e-3
+    res = {"xi": ([], []), "table": ([], []), "table_h1e-5": ([], [])}
+    t0 = time.perf_counter()
+    for i in range(n_dirs):
+        if i % 2 == 0:
+            ux = torch.as_tensor(rng.standard_normal(n), device=dev)
+            ux /= torch.linalg.norm(ux)
+            uv = torch.zeros_like(V64)
+            runs = (("xi", h),)
+        else:
+            ux = torch.zeros_like(xi64)
+            uv = torch.as_tensor(1e-3 * vals * rng.standard_normal(len(vals)), device=dev)
+            runs = (("table", h), ("table_h1e-5", 1e-5))
+        a32 = float(gx32 @ ux + gv32 @ uv)
+        a64 = float(gx64 @ ux + gv64 @ uv)
+        for name, hh in runs:
+            fd = (loss64(xi64 + hh * ux, V64 + hh * uv) - loss64(xi64 - hh * ux, V64 - hh * uv)) / (2 * hh)
+            scale = max(abs(fd), 1e-30)
+            res[name][0].append(abs(a32 - fd) / scale)
+            res[name][1].append(abs(a64 - fd) / scale)
+    fd_s = time.perf_counter() - t0
+
+    def stats(v):
+        return {"max": float(np.max(v)), "median": float(np.median(v)), "count": len(v)} if v else None
+
+    return {"workload": "differentiation: N = 4,194,304 uniform [0,1]^2, n0 = 256, k = 20, RBF scale 0.1, "
+                        "r = 0 + 1,000 log bins on [1e-5, 1.5], jitter 1e-4; loss 0.5|generate(xi) - y|^2 + logdet",
+            "value": n / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
+            "step": "FP32 generate + residual + adjoint (grad w.r.t. 4,194,304 xi and 1,001 table values)",
+            "status_error": st["error"] if st else None, "fallback_points": st["fallback_count"] if st else None,
+            "fd_directions": n_dirs, "fd_step": h,
+            "fd_rel_err_fp32_adjoint": {k: stats(v[0]) for k, v in res.items()},
+            "fd_rel_err_fp64_adjoint": {k: stats(v[1]) for k, v in res.items()},
+            "grad_fp32_vs_fp64_rel": {"xi": float(torch.linalg.norm(gx32 - gx64) / torch.linalg.norm(gx64)),
+                                      "table": float(torch.linalg.norm(gv32 - gv64) / torch.linalg.norm(gv64))},
+            "fd_seconds": fd_s}
 
 
 def serving(dev, n_requests):
@@ -515,6 +609,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the FP64 comparators and CPU baseline")
     ap.add_argument("--ref-sample", type=int, default=200000)
     ap.add_argument("--serving-requests", type=int, default=4096, help="0 skips the serving stream")
+    ap.add_argument("--fd-directions", type=int, default=64,
+                    help="finite-difference directions of the differentiation workload (0 skips it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()

@@ -193,9 +193,8 @@ template <typename T>
 int run_cond(RefineParams<T> p, int mode, int nb, cudaStream_t s) {
   p.mode = mode;
   if (p.n_batches < 1 || p.n == p.n0) return GGP_OK;
-  // generate waits batch on batch: cap its width (4 warps per block is the smaller block of the fast kernels)
-  const int cap = (mode == kGenerate) ? dataflow_blocks(p.n, p.n0, p.n_batches, 4) : 0;
-  return cuda_status(dispatch<T>(p, kCond, nb, cap, s));
+  // generate waits batch on batch: -1 lets the launcher cap its width for the block size it picks
+  return cuda_status(dispatch<T>(p, kCond, nb, mode == kGenerate ? -1 : 0, s));
 }
 
 template <typename T>

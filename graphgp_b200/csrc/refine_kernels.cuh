@@ -37,7 +37,9 @@ struct RefineParams {
 
 // Rows per work chunk of a batch: 8 for small batches (their latency is on the critical path of
 // generate), 32 for large ones (fewer tickets).
-__host__ __device__ __forceinline__ int chunk_rows(long long batch_size) { return batch_size < 16384 ? 8 : 32; }
+// Rows per work chunk (one warp, 8 points). Eight for every batch size: in generate a warp factors all the
+// points of its chunk before it waits, which larger chunks would serialise behind each wait.
+__host__ __device__ __forceinline__ int chunk_rows(long long) { return 8; }
 
 // Block cap for a dependency-ordered launch over rows [n0, n) in n_batches batches: dataflow_width() warps per
 // average chunk of a batch (at least 8 warps), as blocks of warps_per_block; 0 = no cap.

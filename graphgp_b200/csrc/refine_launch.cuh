@@ -21,17 +21,27 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
   if constexpr (K <= 20) {
     RefineParams<T> q = p;
     q.table_smem = (int)((table_smem_bytes<T>(nb) + 255) / 256 * 256);
-    constexpr int kBlock = 256;
-    const size_t smem = q.table_smem + sizeof(T) * (kBlock / 32) * 8 * QuadSmem<K, D>::kPerPoint;
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    // as many warps (up to the launch bound) as the shared memory left by the table holds
+    const size_t per_warp = sizeof(T) * 8 * QuadSmem<K, D>::kPerPoint;
+    long warps = ((long)optin - q.table_smem) / (long)per_warp;
+    if (warps > Quad2Block<T>::kMax / 32) warps = Quad2Block<T>::kMax / 32;
+    if (warps < 1) return launch_generic<T>(p, kind, max_blocks < 0 ? 0 : max_blocks, s);
+    const int block = (int)warps * 32;
+    const size_t smem = q.table_smem + per_warp * warps;
     auto kern = (kind == kCond) ? refine_quad2_kernel<T, K, D, PAD, false> : refine_quad2_kernel<T, K, D, PAD, true>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    int grid = persistent_grid(kern, kBlock, smem, 0);
+    if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, block / 32);
+    int grid = persistent_grid(kern, block, smem, 0);
     if (max_blocks > 0 && grid > max_blocks) grid = max_blocks;
-    (ggp::count_launch(), kern<<<grid, kBlock, smem, s>>>(q));
+    (ggp::count_launch(), kern<<<grid, block, smem, s>>>(q));
     return cudaGetLastError();
   }
   const size_t smem = table_smem_bytes<T>(nb);
+  if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, 4);
   if (kind == kCond) {
     auto kern = refine_quad_kernel<T, K, D, PAD, false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -48,6 +58,7 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
 
 template <typename T>
 cudaError_t launch_generic(const RefineParams<T>& p, int kind, int max_blocks, cudaStream_t s) {
+  if (max_blocks < 0) max_blocks = 0;
   const size_t smem = generic_smem_bytes(p.k, p.d);
   auto kern = refine_generic_kernel<T>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

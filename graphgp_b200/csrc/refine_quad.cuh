@@ -16,8 +16,8 @@
 // entries by rsqrt(pivot), keeping that reciprocal in its diagonal slot for the back substitution. A quad
 // holds about a quarter of the triangle in registers.
 //
-// Work unit: a chunk of `rows_per_chunk` (a multiple of 8) consecutive rows of one depth batch, taken by
-// one warp as 8 points at a time. Chunks are numbered batch after batch and handed out by a global
+// Work unit: a chunk of 8 consecutive rows of one depth batch (chunk_rows), taken by one warp as 8 points. A
+// warp factors its 8 points and only then waits, so no factorisation sits between a wait and the next. Chunks are numbered batch after batch and handed out by a global
 // ticket, so every neighbour of a chunk (an earlier batch) belongs to an earlier ticket held by a running
 // warp: the bounded waits on pending neighbour values always make progress.
 #pragma once
@@ -344,12 +344,49 @@ template <int K, int D> struct QuadSmem {
   static constexpr int kPerPoint = (K + 1) * kPointStride + kPairs + 1;  // +1 staggers banks
 };
 
-// quad_factor with the off-diagonal covariances read from `tri` (pair (i, j), i > j, at i(i-1)/2 + j).
+// Block size of the two-phase kernel: its launch bound (FP32: 20 warps at up to 96 registers, one block per
+// SM; FP64: 8 warps); the launch uses fewer warps when the table leaves too little shared memory.
+template <typename T> struct Quad2Block { static constexpr int kMax = sizeof(T) == 4 ? 640 : 256; };
+
+// Pair covariances of a point into tri[p] (p = i(i-1)/2 + j), dealt p = g, g+4, ... over the quad; pairs with
+// a padding slot (PAD, index >= kk) are 0.
+template <typename T, int K, int D, bool PAD>
+__device__ __forceinline__ void quad_pairs(const T* __restrict__ crd, T* __restrict__ tri, int g, int kk,
+                                           const TableView<T>& tab) {
+  using SM = QuadSmem<K, D>;
+  int i = 1, j = g;
+  while (j >= i) { j -= i; ++i; }
+  for (int pp = g; pp < SM::kPairs; pp += kQuad) {
+    T a = T(0);
+    if (!(PAD && ((i < K && i >= kk) || j >= kk))) {
+      T pi[D], pj[D];
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        pi[c] = crd[i * SM::kPointStride + c];
+        pj[c] = crd[j * SM::kPointStride + c];
+      }
+      a = tab(point_distance<T, D>(pi, pj));
+    }
+    tri[pp] = a;
+    j += kQuad;
+    while (j >= i && i <= K) { j -= i; ++i; }
+  }
+}
+
+// quad_factor with the off-diagonal covariances read from `tri` (pair (i, j), i > j, at i(i-1)/2 + j). Slot t of
+// this lane holds row i = 4t + g; for t > j / 4 every lane's row is below the diagonal of column j, so only
+// the slot holding the diagonal and the last slot (rows past K) need a per-lane test.
 template <typename T, int K>
 __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g, int src0, T c0,
                                                 T (&wmine)[QuadRows<K>::NT], T& var, T& min_ratio) {
   constexpr int R = K + 1;
   constexpr int NT = QuadRows<K>::NT;
+  const T* trow[NT];  // pair row of this lane's row i: tri + i(i-1)/2
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    const int i = t * kQuad + g;
+    trow[t] = tri + (i * (i - 1)) / 2;
+  }
   T L[NT][K + 1];
 #pragma unroll
   for (int t = 0; t < NT; ++t)
@@ -360,17 +397,19 @@ __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g
   T var_out = T(0);
 #pragma unroll
   for (int j = 0; j <= K; ++j) {
-    const int o = j % kQuad;
     const int tj = j / kQuad;
-    const int src = src0 + o;
+    const int src = src0 + j % kQuad;
     T acc[NT];
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       const int i = t * kQuad + g;
       T a = T(0);
-      if (t * kQuad + kQuad - 1 >= j) {
+      if (t > tj) {
+        if (t * kQuad + kQuad - 1 <= K) a = trow[t][j];  // every row of the slot is a point row
+        else if (i <= K) a = trow[t][j];
+      } else if (t == tj) {
         if (i == j) a = c0;
-        else if (i > j && i <= K) a = tri[i * (i - 1) / 2 + j];
+        else if (i > j && i <= K) a = trow[t][j];
       }
       acc[t] = a;
     }
@@ -379,7 +418,7 @@ __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g
       const T b = __shfl_sync(0xffffffffu, L[tj][m], src);
 #pragma unroll
       for (int t = 0; t < NT; ++t)
-        if (t * kQuad + kQuad - 1 >= j) acc[t] = fma(-L[t][m], b, acc[t]);
+        if (t >= tj) acc[t] = fma(-L[t][m], b, acc[t]);
     }
     const T s = __shfl_sync(0xffffffffu, acc[tj], src);
     mr = fmin(mr, s * inv_c0);
@@ -388,7 +427,12 @@ __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       const int i = t * kQuad + g;
-      if (t * kQuad + kQuad - 1 >= j) L[t][j] = (i > j && i < R) ? acc[t] * r : (i == j ? r : L[t][j]);
+      if (t > tj) {
+        if (t * kQuad + kQuad - 1 < R) L[t][j] = acc[t] * r;
+        else L[t][j] = (i < R) ? acc[t] * r : T(0);
+      } else if (t == tj) {
+        L[t][j] = (i > j && i < R) ? acc[t] * r : (i == j ? r : L[t][j]);
+      }
     }
   }
   quad_backsub<T, K>(L, g, src0, wmine);
@@ -397,11 +441,12 @@ __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g
 }
 
 template <typename T, int K, int D, bool PAD, bool LOGDET>
-__global__ void __launch_bounds__(256) refine_quad2_kernel(RefineParams<T> p) {
+__global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(RefineParams<T> p) {
   constexpr int NT = QuadRows<K>::NT;
   using SM = QuadSmem<K, D>;
   extern __shared__ __align__(32) unsigned char smem[];
-  __shared__ double s_part[8];
+  __shared__ double s_part[Quad2Block<T>::kMax / 32];
+  // shared memory: table | per-warp point scratch (8 points per warp)
   const TableView<T> tab = stage_table<T>(p.tb, smem);
   const int warp = threadIdx.x >> 5;
   T* scratch = reinterpret_cast<T*>(smem + p.table_smem) + (size_t)warp * 8 * SM::kPerPoint;
@@ -443,27 +488,8 @@ __global__ void __launch_bounds__(256) refine_quad2_kernel(RefineParams<T> p) {
         }
       }
       __syncwarp();
-      // phase 1: covariances of all pairs i > j, pair index p = i(i-1)/2 + j, dealt p = g, g+4, ...
-      {
-        int i = 1, j = g;
-        while (j >= i) { j -= i; ++i; }
-        const int kk = p.k;
-        for (int pp = g; pp < SM::kPairs; pp += kQuad) {
-          T a = T(0);
-          if (!(PAD && ((i < K && i >= kk) || j >= kk))) {
-            T pi[D], pj[D];
-#pragma unroll
-            for (int c = 0; c < D; ++c) {
-              pi[c] = crd[i * SM::kPointStride + c];
-              pj[c] = crd[j * SM::kPointStride + c];
-            }
-            a = tab(point_distance<T, D>(pi, pj));
-          }
-          tri[pp] = a;
-          j += kQuad;
-          while (j >= i && i <= K) { j -= i; ++i; }
-        }
-      }
+      // phase 1: covariances of all pairs i > j, dealt p = g, g+4, ...
+      quad_pairs<T, K, D, PAD>(crd, tri, g, p.k, tab);
       __syncwarp();
       T wmine[NT], var, mr;
       quad_factor_tri<T, K>(tri, g, src0, c0, wmine, var, mr);

@@ -213,8 +213,15 @@ struct TableView {
   // above bins[-1] the last bracket gives vals[-1] up to one rounding (jnp.interp's end values).
   __device__ __forceinline__ T operator()(T r) const {
     r = fmin(fmax(r, b0), blast);
-    long long c = radius_key(r, shift) - key_lo;
-    c = c < 0 ? 0 : (c >= n_hint ? n_hint - 1 : c);
+    int c;
+    if constexpr (sizeof(T) == 4) {
+      // r >= 0 is finite here, so its bit pattern is below 2^31: 32-bit key arithmetic is exact
+      c = (int)(__float_as_uint(r) >> shift) - (int)key_lo;
+      c = min(max(c, 0), n_hint - 1);
+    } else {
+      long long cl = radius_key(r, shift) - key_lo;
+      c = (int)(cl < 0 ? 0 : (cl >= n_hint ? n_hint - 1 : cl));
+    }
     int j = hint[c];
     Bracket<T> e = br[j];
     if (max_steps <= 2) {

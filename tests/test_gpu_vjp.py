@@ -94,3 +94,34 @@ def test_vjp_finite_differences_on_gpu(cuda_device):
         fd = (loss(xi + h * dx, vals + h * dv) - loss(xi - h * dx, vals - h * dv)) / (2 * h)
         an = float(gx @ dx + gvals @ dv)
         assert abs(fd - an) <= 1e-5 * max(1.0, abs(fd))
+
+
+def test_vjp_differentiation_workload_shape(cuda_device):
+    """The differentiation workload's shape at N = 20,000: uniform [0,1]^2, n0 = 256, k = 20, RBF scale 0.1 on
+    r = 0 + 1,000 log bins over [1e-5, 1.5], jitter 1e-4, loss 0.5|v - y|^2 + logdet. GPU adjoint (FP64 and
+    FP32) against the oracle adjoint."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+    from oracle import extras as ox
+    from oracle import graph as og
+    from oracle import refine as orf
+
+    n = 20000
+    rng = np.random.default_rng(77)
+    pts = rng.uniform(0.0, 1.0, (n, 2)).astype(np.float32)
+    g = og.build_graph(pts, n0=256, k=20)
+    bins, vals = ox.rbf_kernel(variance=1.0, scale=0.1, r_min=1e-5, r_max=1.5, n_bins=1001, jitter=1e-4)
+    y = orf.generate(g, (bins, vals), rng.standard_normal(n)) + 0.01 * rng.standard_normal(n)
+    xi = rng.standard_normal(n)
+    v = orf.generate(g, (bins, vals), xi)
+    rx, rv = oa.generate_vjp(g, (bins, vals), xi, v - y, 1.0)
+    args = (_t(g.indices, cuda_device), _t(g.neighbors, cuda_device), g.offsets)
+    for dt, tol_x, tol_v in ((torch.float64, 1e-8, 1e-8), (torch.float32, 1e-4, 1e-3)):
+        P = _t(g.points, cuda_device, dt)
+        B, V = _t(bins, cuda_device, dt), _t(vals, cuda_device, dt)
+        X = _t(xi, cuda_device, dt)
+        vg = gc.generate(P, *args, B, V, X)
+        gx, gvals = gc.generate_vjp(P, *args, B, V, X, vg - _t(y, cuda_device, dt), 1.0)
+        assert gc.last_status()["error"] == 0
+        assert rel_err(gx.cpu().numpy(), rx) < tol_x, dt
+        assert rel_err(gvals.cpu().numpy(), rv) < tol_v, dt
