@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
 
 // Launch bound of the four-lane adjoint kernel; the launch may use smaller blocks (a multiple of 32 threads)
 // when the table and histogram leave too little shared memory.
-template <typename T> struct VjpQuadBlock { static constexpr int kMax = sizeof(T) == 4 ? 512 : 256; };
+template <typename T> struct VjpQuadBlock { static constexpr int kMax = sizeof(T) == 4 ? 640 : 256; };
 
 // Returns cudaErrorInvalidConfiguration, launching nothing, when even one warp's scratch does not fit.
 template <typename T, int K, int D, bool PAD>
