@@ -6,9 +6,11 @@
 namespace ggp {
 
 // depth[i] = 0 for i < n0, else 1 + max(depth[nbrs]) (graph.py:101-120: the Jacobi fixed point, which for a
-// topologically ordered graph is this single pass). Warps take chunks of 32 rows in row order; a row waits
-// (bounded) for neighbours before its chunk, which belong to earlier tickets; neighbours inside the chunk
-// are resolved by iterating max-plus updates over warp shuffles until nothing changes.
+// topologically ordered graph is this single pass). Warps take chunks of 32 rows in row order and each lane
+// waits (bounded) for its own row's neighbours, then stores its depth at once: a neighbour before the chunk
+// belongs to an earlier ticket, one inside it to a lower lane of the same warp, so every wait ends. Storing
+// per lane (rather than once the whole chunk is settled) keeps a shallow row from inheriting the delay of the
+// deepest row of its chunk.
 __global__ void __launch_bounds__(256) depths_kernel(const int* __restrict__ nbrs, long long n, long long n0, int k,
                                                      int* __restrict__ depth, DeviceStatus* st,
                                                      unsigned long long timeout_ns) {
@@ -27,39 +29,28 @@ __global__ void __launch_bounds__(256) depths_kernel(const int* __restrict__ nbr
       for (int m = 0; m < k; ++m) {
         const int id = nr[m];
         if (id < 0 || (long long)id >= row) { bad = true; continue; }
-        if ((long long)id < cs) {
-          int v = ld_relaxed(depth + id);
-          if (v < 0) {
-            const uint64_t t0 = global_timer_ns();
-            unsigned int backoff = 32;
-            while (v < 0) {
-              __nanosleep(backoff);
-              if (backoff < 512) backoff <<= 1;
-              v = ld_relaxed(depth + id);
-              if (v < 0 && global_timer_ns() - t0 > timeout_ns) {
-                atomicAdd(&st->timeouts, 1u);
-                report_error(st, GGP_ERR_TIMEOUT);
-                v = 0;
-              }
+        // a neighbour inside this chunk is a lower lane of this warp, which stores its depth as soon as it is
+        // known; the divergent lanes of a warp progress independently, and every wait is bounded
+        int v = ld_relaxed(depth + id);
+        if (v < 0) {
+          const uint64_t t0 = global_timer_ns();
+          unsigned int backoff = 32;
+          while (v < 0) {
+            __nanosleep(backoff);
+            if (backoff < 512) backoff <<= 1;
+            v = ld_relaxed(depth + id);
+            if (v < 0 && global_timer_ns() - t0 > timeout_ns) {
+              atomicAdd(&st->timeouts, 1u);
+              report_error(st, GGP_ERR_TIMEOUT);
+              v = 0;
             }
           }
-          ext = v > ext ? v : ext;
         }
+        ext = v > ext ? v : ext;
       }
     }
     if (bad) report_error(st, GGP_ERR_INVALID);
-    int my = ext + 1;
-    for (int it = 0; it < 33; ++it) {
-      bool changed = false;
-      for (int m = 0; m < k; ++m) {
-        const int id = valid ? nr[m] : -1;
-        const bool inside = valid && (long long)id >= cs && (long long)id < row;
-        const int srcl = inside ? (int)(id - cs) : lane;
-        const int v = __shfl_sync(0xffffffffu, my, srcl);
-        if (inside && v + 1 > my) { my = v + 1; changed = true; }
-      }
-      if (!__any_sync(0xffffffffu, changed)) break;
-    }
+    const int my = ext + 1;
     if (valid) st_relaxed(depth + row, my);
   }
 }
