@@ -204,10 +204,18 @@ template <typename T, int D>
 static cudaError_t launch_knn_d(const PointSource<T, D>& src, long long n, int k, const int* q, const int* m,
                                 long long nq, long long q0, int* out, cudaStream_t s) {
   const int grid = g_grid(nq, 128);
-  if (k <= 8) (ggp::count_launch(), knn_kernel<T, D, 8><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
-  else if (k <= 16) (ggp::count_launch(), knn_kernel<T, D, 16><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
-  else if (k <= 32) (ggp::count_launch(), knn_kernel<T, D, 32><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
-  else (ggp::count_launch(), knn_kernel_wide<T, D><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+  const bool idx32 = n < (1ll << 30);  // 32-bit tree indices
+  if (k > 32) {
+    (ggp::count_launch(), knn_kernel_wide<T, D><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+  } else if (idx32) {
+    if (k <= 8) (ggp::count_launch(), knn_kernel<T, D, 8, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+    else if (k <= 16) (ggp::count_launch(), knn_kernel<T, D, 16, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+    else (ggp::count_launch(), knn_kernel<T, D, 32, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+  } else {
+    if (k <= 8) (ggp::count_launch(), knn_kernel<T, D, 8, long long><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+    else if (k <= 16) (ggp::count_launch(), knn_kernel<T, D, 16, long long><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+    else (ggp::count_launch(), knn_kernel<T, D, 32, long long><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+  }
   return cudaGetLastError();
 }
 

@@ -83,9 +83,20 @@ __device__ __forceinline__ T coord(const T* p, int s) {
 
 constexpr int kKnnMaxD = 16;
 
+// Tree index arithmetic of the traversal in 64 bits, or in 32 bits when n < 2^30 (then every index, child
+// index included, stays below 2^31).
+__device__ __forceinline__ int tree_level(long long j1) { return 63 - __clzll(j1); }
+__device__ __forceinline__ int tree_level(int j1) { return 31 - __clz(j1); }
+__device__ __forceinline__ int tree_parent(int j) {
+  if (j == 0) return -1;
+  const int lvl = 31 - __clz(j + 1);
+  const int n_above = (1 << lvl) - 1, npl = 1 << (lvl - 1);
+  return j < n_above + npl ? j - npl : j - 2 * npl;
+}
+
 // KMAX: compile-time slot capacity (registers for KMAX <= 32); k <= KMAX at run time.
 // Queries: query_idx / max_idx arrays, or (when null) rows q0 + t with max index = the row itself.
-template <typename T, int D, int KMAX>
+template <typename T, int D, int KMAX, typename IDX>
 __global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long long n, int k,
                                                   const int* __restrict__ query_idx, const int* __restrict__ max_idx,
                                                   long long nq, long long q0, int* __restrict__ out) {
@@ -108,9 +119,10 @@ __global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long lo
     }
     T maxv = inf;
     int maxj = 0;
-    long long cur = mx > 0 ? 0 : -1, prev = -1;
+    const IDX mxi = (IDX)mx;
+    IDX cur = mx > 0 ? 0 : -1, prev = -1;
     while (cur != -1) {
-      const long long par = tree_parent(cur);
+      const IDX par = tree_parent(cur);
       T p[PD];
       int s;
       src.load(cur, p, s);
@@ -128,13 +140,13 @@ __global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long lo
         }
       }
       const T sd = rn_sub(coord<T, D>(q, s), coord<T, D>(p, s));
-      const int lvl = 63 - __clzll(cur + 1);
-      const long long left = cur + (1ll << lvl), right = cur + (2ll << lvl);
-      const long long nearc = sd < T(0) ? left : right;
-      const long long farc = sd < T(0) ? right : left;
+      const int lvl = tree_level((IDX)(cur + 1));
+      const IDX left = cur + ((IDX)1 << lvl), right = cur + ((IDX)2 << lvl);
+      const IDX nearc = sd < T(0) ? left : right;
+      const IDX farc = sd < T(0) ? right : left;
       const bool far_in = rn_mul(sd, sd) <= maxv;
-      long long next;
-      if (prev == nearc || (prev == par && nearc >= mx)) next = (farc < mx && far_in) ? farc : par;
+      IDX next;
+      if (prev == nearc || (prev == par && nearc >= mxi)) next = (farc < mxi && far_in) ? farc : par;
       else next = (prev == par) ? nearc : par;
       prev = cur;
       cur = next;
@@ -158,15 +170,25 @@ __global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long lo
         nb[j] = 0x7fffffff;
       }
     }
-    // odd-even transposition sort (KMAX passes) on (key, id)
+    // bitonic sorting network on (key, id), ascending (KMAX is a power of two; slots past k hold
+    // (inf, INT_MAX) and sort last). (key, id) pairs are distinct except for identical unfilled slots, so the
+    // order is the same as any other sort's.
+    static_assert((KMAX & (KMAX - 1)) == 0, "bitonic network needs a power-of-two slot count");
 #pragma unroll
-    for (int pass = 0; pass < KMAX; ++pass) {
+    for (int size = 2; size <= KMAX; size <<= 1) {
 #pragma unroll
-      for (int j = (pass & 1); j + 1 < KMAX; j += 2) {
-        const bool sw = (key[j + 1] < key[j]) || (key[j + 1] == key[j] && nb[j + 1] < nb[j]);
-        if (sw) {
-          const T tk = key[j]; key[j] = key[j + 1]; key[j + 1] = tk;
-          const int ti = nb[j]; nb[j] = nb[j + 1]; nb[j + 1] = ti;
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+        for (int i = 0; i < KMAX; ++i) {
+          const int j = i ^ stride;
+          if (j > i) {
+            const bool j_less = (key[j] < key[i]) || (key[j] == key[i] && nb[j] < nb[i]);
+            const bool sw = ((i & size) == 0) ? j_less : !j_less;
+            if (sw) {
+              const T tk = key[i]; key[i] = key[j]; key[j] = tk;
+              const int ti = nb[i]; nb[i] = nb[j]; nb[j] = ti;
+            }
+          }
         }
       }
     }
