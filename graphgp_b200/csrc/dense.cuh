@@ -36,35 +36,45 @@ __global__ void dense_cov_kernel(const TP* __restrict__ points, long long n0, in
   }
 }
 
-// Factor the diagonal tile (p, p) in place.
+// Factor the diagonal tile (p, p) in place. 256 threads as 16 x 16; for each column j the pivot is read by all,
+// the column below it divided by the pivot's square root, and each thread updates the 4 x 4 block of the tile
+// it owns (rows 4ty.., columns 4tx..) where j < m <= i.
 __global__ void __launch_bounds__(256) dense_potrf_tile_kernel(double* __restrict__ A, long long n, int p) {
   __shared__ double t[kDenseTile][kDenseTile + 1];
   const long long o = (long long)p * kDenseTile;
   const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, j = e - i * nb;
-    t[i][j] = A[(o + i) * n + o + j];
-  }
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  for (int r = ty; r < nb; r += 16)
+    for (int c = tx; c < nb; c += 16) t[r][c] = A[(o + r) * n + o + c];
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
     const double djj = sqrt(t[j][j]);
-    __syncthreads();
-    for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) t[i][j] /= djj;
-    if (threadIdx.x == 0) t[j][j] = djj;
-    __syncthreads();
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-      const int i = e / nb, m = e - i * nb;
-      if (m > j && m <= i) t[i][m] -= t[i][j] * t[m][j];
+    __syncthreads();  // every thread has read the pivot before it is overwritten
+    if (tid < nb) {
+      if (tid > j) t[tid][j] /= djj;
+      else if (tid == j) t[j][j] = djj;
     }
     __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = ty * 4 + u;
+      if (i > j && i < nb) {
+        const double lij = t[i][j];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const int m = tx * 4 + v;
+          if (m > j && m <= i) t[i][m] -= lij * t[m][j];
+        }
+      }
+    }
+    __syncthreads();  // the next pivot was just updated
   }
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, j = e - i * nb;
-    A[(o + i) * n + o + j] = (j <= i) ? t[i][j] : 0.0;
-  }
+  for (int r = ty; r < nb; r += 16)
+    for (int c = tx; c < nb; c += 16) A[(o + r) * n + o + c] = (c <= r) ? t[r][c] : 0.0;
 }
 
-// Panel solve: tile rows below p, X L_pp^T = A_ip; one block per tile row, one thread per matrix row.
+// Panel solve: tile rows below p, X L_pp^T = A_ip; one block per tile row, one thread per matrix row, the row's
+// unknowns in registers (compile-time indices).
 __global__ void __launch_bounds__(kDenseTile) dense_trsm_kernel(double* __restrict__ A, long long n, int p) {
   __shared__ double Lp[kDenseTile][kDenseTile + 1];
   const long long o = (long long)p * kDenseTile;
@@ -82,6 +92,7 @@ __global__ void __launch_bounds__(kDenseTile) dense_trsm_kernel(double* __restri
   for (int j = 0; j < kDenseTile; ++j) {
     if (j < nb) {
       double s = row[j];
+#pragma unroll
       for (int m = 0; m < j; ++m) s = fma(-x[m], Lp[j][m], s);
       x[j] = s / Lp[j][j];
     }
