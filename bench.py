@@ -347,7 +347,31 @@ def run_ours(args, world, rank, local):
         line["clocks"] = clk.summary()
         if not args.quick:
             line["cpu_baseline"] = cpu_baseline(gp, gn, offs, bins, vals)
+        if args.largest:
+            del gp, gi, gn, OF, XI, P, out, Y
+            torch.cuda.empty_cache()
+            line["largest"] = largest(dev, n=args.largest_n, steps=1)
         print(json.dumps(line), flush=True)
+
+
+def largest_points(n, seed=2027, block=1 << 20):
+    """Points of the largest-instance workload: a mixture of 64 Gaussian clusters (centres uniform in [-1, 1]^3,
+    per-cluster sigma 10^U(-3, -1), 90 % of the points) plus 10 % uniform background in [-1, 1]^3, float32.
+    Generated in blocks of 2^20 points, block b from seed + 1 + b, so the first 2^20 points (the parity
+    subset) are the same whatever n is."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(-1.0, 1.0, (64, 3))
+    sigmas = 10.0 ** rng.uniform(-3.0, -1.0, 64)
+    out = np.empty((n, 3), np.float32)
+    for b0 in range(0, n, block):
+        m = min(block, n - b0)
+        r = np.random.default_rng(seed + 1 + b0 // block)
+        c = r.integers(0, 64, m)
+        x = centres[c] + sigmas[c, None] * r.standard_normal((m, 3))
+        bg = r.random(m) < 0.1
+        x[bg] = r.uniform(-1.0, 1.0, (int(bg.sum()), 3))
+        out[b0:b0 + m] = x
+    return out
 
 
 def differentiation(dev, n_dirs=64, steps=5, warmup=3, n=4194304):
@@ -440,6 +464,78 @@ def differentiation(dev, n_dirs=64, steps=5, warmup=3, n=4194304):
             "grad_fp32_vs_fp64_rel": {"xi": float(torch.linalg.norm(gx32 - gx64) / torch.linalg.norm(gx64)),
                                       "table": float(torch.linalg.norm(gv32 - gv64) / torch.linalg.norm(gv64))},
             "fd_seconds": fd_s}
+
+
+def largest(dev, n=1 << 28, steps=2):
+    """The largest single instance: 2^28 points (largest_points), d = 3, n0 = 4096, k = 32, RBF scale 0.02 on
+    r = 0 + 4,096 log bins over [1e-7, 4], jitter 1e-5. Times build_graph, generate and generate + adjoint, and
+    checks the graph of the first 2^20 points bit for bit against the oracle's digests
+    (tests/golden/largest_subset.json)."""
+    import hashlib
+
+    import torch
+
+    from graphgp_b200 import extras
+    from graphgp_b200 import graphgp_cuda as gc
+
+    def digest(a):
+        return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+    out = {"workload": "largest instance: 2^28 points (64-cluster Gaussian mixture, sigma 10^U(-3,-1), plus 10% "
+                       "uniform background in [-1,1]^3), d = 3, n0 = 4096, k = 32, RBF scale 0.02, r = 0 + 4,096 "
+                       "log bins on [1e-7, 4], jitter 1e-5", "n_points": n}
+    fx = json.loads(open(os.path.join(ROOT, "tests", "golden", "largest_subset.json")).read())
+    sub = largest_points(fx["n"])
+    gp, gi, gn, _, offs = gc.build_graph(torch.as_tensor(sub, device=dev), n0=fx["n0"], k=fx["k"], return_offsets=True)
+    out["subset_bit_exact"] = bool(list(offs) == fx["offsets"]
+                                   and digest(gi.cpu().numpy().astype(np.int32)) == fx["indices_sha256"]
+                                   and digest(gn.cpu().numpy().astype(np.int32)) == fx["neighbors_sha256"]
+                                   and digest(gp.cpu().numpy().astype(np.float32)) == fx["points_graph_sha256"])
+    del gp, gi, gn
+    t = time.perf_counter()
+    pts = largest_points(n)
+    out["host_generation_s"] = time.perf_counter() - t
+    P = torch.as_tensor(pts, device=dev)
+    del pts
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record()
+    gp, gi, gn, _, offs = gc.build_graph(P, n0=4096, k=32, return_offsets=True)
+    e1.record()
+    torch.cuda.synchronize()
+    out["graph_build_ms"] = e0.elapsed_time(e1)
+    out["batches"] = len(offs) - 1
+    del P
+    torch.cuda.empty_cache()
+    OF = torch.as_tensor(offs, dtype=torch.int32, device=dev)
+    B, V = extras.rbf_kernel(variance=1.0, scale=0.02, r_min=1e-7, r_max=4.0, n_bins=4097, jitter=1e-5, device=dev)
+    xi = torch.randn(n, generator=torch.Generator(device=dev).manual_seed(3), device=dev)
+    v = gc.generate(gp, gi, gn, OF, B, V, xi)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(steps):
+        v = gc.generate(gp, gi, gn, OF, B, V, xi)
+    e1.record()
+    torch.cuda.synchronize()
+    st = gc.last_status()
+    out["generate_ms"] = e0.elapsed_time(e1) / steps
+    out["generate_points_per_s"] = n / (out["generate_ms"] * 1e-3)
+    out["generate_status"] = st
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(steps):
+        v = gc.generate(gp, gi, gn, OF, B, V, xi)
+        gx, gv = gc.generate_vjp(gp, gi, gn, OF, B, V, xi, v, 0.5)
+    e1.record()
+    torch.cuda.synchronize()
+    out["generate_grad_ms"] = e0.elapsed_time(e1) / steps
+    out["generate_grad_points_per_s"] = n / (out["generate_grad_ms"] * 1e-3)
+    out["vjp_status"] = gc.last_status()
+    out["finite"] = bool(torch.isfinite(v).all() and torch.isfinite(gx).all() and torch.isfinite(gv).all())
+    out["peak_device_gb"] = torch.cuda.max_memory_allocated(dev) / 1e9
+    return out
 
 
 def serving(dev, n_requests):
@@ -609,6 +705,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the FP64 comparators and CPU baseline")
     ap.add_argument("--ref-sample", type=int, default=200000)
     ap.add_argument("--serving-requests", type=int, default=4096, help="0 skips the serving stream")
+    ap.add_argument("--largest", action="store_true", help="also run the 2^28-point largest instance")
+    ap.add_argument("--largest-n", type=int, default=1 << 28)
     ap.add_argument("--fd-directions", type=int, default=64,
                     help="finite-difference directions of the differentiation workload (0 skips it)")
     args = ap.parse_args()

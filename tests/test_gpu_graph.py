@@ -192,3 +192,32 @@ def test_build_graph_vs_oracle(cuda_device, n, d, n0, k):
     assert np.array_equal(_np(nb), g.neighbors)
     assert offs == g.offsets
     og.check_graph(og.Graph(_np(p), _np(nb), offs, _np(i)))
+
+
+def test_largest_instance_subset_bit_exact(cuda_device):
+    """The largest-instance workload's parity subset (its first 2^20 points: 64-cluster Gaussian mixture plus
+    uniform background, d = 3, n0 = 4096, k = 32): the GPU graph (indices, neighbours, ordered points,
+    offsets) equals the oracle's bit for bit, compared through the SHA-256 digests that
+    tests/golden/make_largest_subset.py recorded from the oracle."""
+    import hashlib
+    import json
+    from pathlib import Path
+
+    import torch
+
+    from bench import largest_points
+    from graphgp_b200 import graphgp_cuda as gc
+
+    fx = json.loads((Path(__file__).parent / "golden" / "largest_subset.json").read_text())
+
+    def digest(a):
+        return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+    pts = largest_points(fx["n"])
+    assert digest(pts) == fx["points_sha256"]
+    gp, gi, gn, _, offs = gc.build_graph(torch.as_tensor(pts, device=cuda_device), n0=fx["n0"], k=fx["k"],
+                                         return_offsets=True)
+    assert list(offs) == fx["offsets"]
+    assert digest(gi.cpu().numpy().astype(np.int32)) == fx["indices_sha256"]
+    assert digest(gn.cpu().numpy().astype(np.int32)) == fx["neighbors_sha256"]
+    assert digest(gp.cpu().numpy().astype(np.float32)) == fx["points_graph_sha256"]
