@@ -1,14 +1,16 @@
 // Adjoint of generate: gradients of <g, generate(xi)> + g_logdet * generate_logdet with respect to xi and the
 // table values (what JAX autodiff computes through reference graphgp/refine.py:21-76, 123-145).
 //
-// Reverse sweep, one thread per refined point, batches from last to first in one persistent kernel: warps
-// take chunks in reverse dependency order from a ticket, and a chunk of batch b starts only once every chunk
-// of the later batches has finished (a global completion counter; those chunks hold earlier tickets, so the
-// bounded wait always ends). A point then owns its final cotangent vbar_i: it recomputes its covariance and
-// Cholesky factor from the table (nothing is stored between the passes), forms w = K11^-1 k12 and
-// a = K11^-1 v_N, writes xibar_i = sigma_i vbar_i, scatters w_m vbar_i into its neighbours' cotangents, and
-// adds the derivative of (mean, sigma) with respect to every covariance entry to a per-block FP64 histogram
-// over the table brackets (jnp.interp is linear in the table values: weights 1 - t and t).
+// Reverse sweep, one thread per refined point (the general kernel, k <= 32 and d <= 8; vjp_quad.cuh is the
+// four-lane kernel for k <= 20, d in {2, 3}), batches from last to first in one persistent kernel: groups of 8
+// lanes take chunks in reverse dependency order from a ticket, and the cotangent of a chunk of batch b is
+// final once every chunk of the later batches has finished (a global completion counter; those chunks hold
+// earlier tickets, so the bounded wait always ends). Before that wait a point recomputes its covariance and
+// Cholesky factor from the table (nothing is stored between the passes) and forms w = K11^-1 k12 and
+// a = K11^-1 v_N; after it, it writes xibar_i = sigma_i vbar_i and scatters w_m vbar_i into its neighbours'
+// cotangents, counts its chunk as finished, and only then adds the derivative of (mean, sigma) with respect to
+// every covariance entry to a per-block FP64 histogram over the table brackets (jnp.interp is linear in the
+// table values: weights 1 - t and t).
 #pragma once
 
 #include "vjp_common.cuh"
@@ -28,39 +30,38 @@ __global__ void __launch_bounds__(128) vjp_refine_kernel(VjpParams<T> v) {
   T t0;
   locate(tab, T(0), j0, t0);  // bracket of r = 0: every diagonal entry
   const int lane = threadIdx.x & 31;
+  // groups of 8 lanes (one chunk of chunk_rows() = 8 rows, one row per lane) take tickets independently; the
+  // divergent groups of a warp progress independently, so a group may wait on a chunk another group holds
+  const int gl = lane & 7;
+  const int leader = lane & ~7;
+  const unsigned int gmask = 0xffu << leader;
   const int k = p.k, d = p.d;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
+  bool waited_out = false;
   for (;;) {
-    const unsigned int tk = warp_ticket(&p.status->ticket2);
+    unsigned int tk = 0;
+    if (gl == 0) tk = atomicAdd(&p.status->ticket2, 1u);
+    tk = __shfl_sync(gmask, tk, leader);
     if (tk >= total) break;
     const unsigned int rc = total - 1 - tk;  // chunks in reverse order
     const int b = find_batch(p.chunk_prefix, p.n_batches, rc);
     // every chunk of batches after b must be finished: those are the first (total - prefix[b+1]) tickets
     const unsigned int need = total - (unsigned int)__ldg(p.chunk_prefix + b + 1);
-    if (lane == 0) {
-      const uint64_t t_start = global_timer_ns();
-      unsigned int backoff = 32;
-      while ((unsigned int)ld_acquire_u32(&p.status->done) < need) {
-        __nanosleep(backoff);
-        if (backoff < 512) backoff <<= 1;
-        if (global_timer_ns() - t_start > p.timeout_ns) {
-          atomicAdd(&p.status->timeouts, 1u);
-          report_error(p.status, GGP_ERR_TIMEOUT);
-          break;
-        }
-      }
-    }
-    __syncwarp();
     long long bstart = (long long)__ldg(p.offsets + b);
     bstart = bstart < p.n0 ? p.n0 : bstart;
     long long end = __ldg(p.offsets + b + 1);
     end = end > p.n ? p.n : end;
     const int rpc = chunk_rows((long long)__ldg(p.offsets + b + 1) - (long long)__ldg(p.offsets + b));
-    const long long row = bstart + (long long)(rc - (unsigned int)__ldg(p.chunk_prefix + b)) * rpc + lane;
-    if (lane < rpc && row < end) {
-      const long long r0 = row - p.n0;
-      int ids[kVjpMaxK];
-      T P[kVjpMaxK + 1][kVjpMaxD];
+    const long long row = bstart + (long long)(rc - (unsigned int)__ldg(p.chunk_prefix + b)) * rpc + gl;
+    const bool active = gl < rpc && row < end;
+    const long long r0 = row - p.n0;
+    // before the wait: covariance, Cholesky factor, z = L11^-1 vN, w = L11^-T l21, a = L11^-T z (the forward
+    // values vN are final; only this point's cotangent is not)
+    int ids[kVjpMaxK];
+    T P[kVjpMaxK + 1][kVjpMaxD];
+    T w[kVjpMaxK], a[kVjpMaxK];
+    T sig = T(1);
+    if (active) {
       T vN[kVjpMaxK];
       for (int m = 0; m < k; ++m) {
         int id = __ldg(p.nbrs + r0 * k + m);
@@ -73,8 +74,7 @@ __global__ void __launch_bounds__(128) vjp_refine_kernel(VjpParams<T> v) {
         vN[m] = p.values[id];
       }
       for (int c = 0; c < d; ++c) P[k][c] = __ldg(p.points + row * d + c);
-      // covariance (packed lower, rows 0..k) and its Cholesky factor in place
-      T A[(kVjpMaxK + 1) * (kVjpMaxK + 2) / 2];
+      T A[(kVjpMaxK + 1) * (kVjpMaxK + 2) / 2];  // packed lower, rows 0..k
       for (int i = 0; i <= k; ++i) {
         T* ri = A + i * (i + 1) / 2;
         for (int j = 0; j < i; ++j) {
@@ -97,15 +97,15 @@ __global__ void __launch_bounds__(128) vjp_refine_kernel(VjpParams<T> v) {
         }
       }
       const T* lk = A + k * (k + 1) / 2;  // row k: l21, then sigma
-      const T sig = lk[k];
-      T z[kVjpMaxK], w[kVjpMaxK], a[kVjpMaxK];
-      for (int i = 0; i < k; ++i) {  // z = L11^-1 vN
+      sig = lk[k];
+      T z[kVjpMaxK];
+      for (int i = 0; i < k; ++i) {
         const T* ri = A + i * (i + 1) / 2;
         T s = vN[i];
         for (int m = 0; m < i; ++m) s = fma(-ri[m], z[m], s);
         z[i] = s / ri[i];
       }
-      for (int i = k - 1; i >= 0; --i) {  // w = L11^-T l21, a = L11^-T z
+      for (int i = k - 1; i >= 0; --i) {
         T sw = lk[i], sa = z[i];
         for (int m = i + 1; m < k; ++m) {
           const T lmi = A[m * (m + 1) / 2 + i];
@@ -116,14 +116,40 @@ __global__ void __launch_bounds__(128) vjp_refine_kernel(VjpParams<T> v) {
         w[i] = sw / lii;
         a[i] = sa / lii;
       }
-      const T vb = ld_relaxed(v.vbar + row);
-      const long long uo = p.perm ? (long long)__ldg(p.perm + row) : row;
+    }
+    // the wait (group leader), then the O(k) part on the dependency chain
+    if (gl == 0 && !waited_out) {
+      const uint64_t t_start = global_timer_ns();
+      unsigned int backoff = 32;
+      while ((unsigned int)ld_acquire_u32(&p.status->done) < need) {
+        __nanosleep(backoff);
+        if (backoff < 512) backoff <<= 1;
+        if (global_timer_ns() - t_start > p.timeout_ns) {
+          atomicAdd(&p.status->timeouts, 1u);
+          report_error(p.status, GGP_ERR_TIMEOUT);
+          waited_out = true;
+          break;
+        }
+      }
+    }
+    __syncwarp(gmask);
+    T vb = T(0);
+    long long uo = 0;
+    if (active) {
+      vb = ld_relaxed(v.vbar + row);
+      uo = p.perm ? (long long)__ldg(p.perm + row) : row;
+      v.grad_xi[uo] = canonical(sig * vb);
+      for (int m = 0; m < k; ++m) atomicAdd(v.vbar + ids[m], w[m] * vb);
+    }
+    // publish this chunk: its cotangent scatters before the completion count
+    __threadfence();
+    __syncwarp(gmask);
+    if (gl == 0) atomicAdd(&p.status->done, 1u);
+    // off the chain: d(mean, sigma) / d(covariance entries) -> table brackets
+    if (active) {
       const T xi = p.perm ? __ldg(p.xi + uo) : __ldg(p.xi + r0);
       const double mb = (double)vb;
       const double sb = (double)vb * (double)xi + v.g_logdet / (double)sig;
-      v.grad_xi[uo] = canonical(sig * vb);
-      for (int m = 0; m < k; ++m) atomicAdd(v.vbar + ids[m], w[m] * vb);
-      // d(mean, sigma) / d(covariance entries) -> table brackets
       const double is = 1.0 / (double)sig;
       double diag = sb * 0.5 * is;  // K22
       for (int i = 0; i < k; ++i) {
@@ -153,10 +179,6 @@ __global__ void __launch_bounds__(128) vjp_refine_kernel(VjpParams<T> v) {
       }
       hist_add(hist, j0, diag, (double)t0, v.nb);
     }
-    // publish this chunk: its cotangent scatters before the completion count
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) atomicAdd(&p.status->done, 1u);
   }
   __syncthreads();
   double* out = v.hist_partials + (size_t)blockIdx.x * v.nb;

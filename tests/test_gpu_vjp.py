@@ -125,3 +125,27 @@ def test_vjp_differentiation_workload_shape(cuda_device):
         assert gc.last_status()["error"] == 0
         assert rel_err(gx.cpu().numpy(), rx) < tol_x, dt
         assert rel_err(gvals.cpu().numpy(), rv) < tol_v, dt
+
+
+# shapes outside the four-lane kernel (k > 20, or d not in {2, 3}): the one-thread-per-point adjoint kernel
+GENERAL_CASES = [(1500, 2, 64, 24, "rbf", 0.3), (1200, 4, 64, 10, "matern", 0.0), (1000, 3, 64, 32, "matern", -0.4)]
+
+
+@pytest.mark.parametrize("n,d,n0,k,tab,gl", GENERAL_CASES)
+def test_vjp_general_kernel_vs_oracle(cuda_device, n, d, n0, k, tab, gl):
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    pts, g = oracle_graph(n, d, n0, k)
+    bins, vals = _table(tab)
+    rng = np.random.default_rng(n + 3 * k)
+    xi, gv = rng.standard_normal(n), rng.standard_normal(n)
+    rx, rv = oa.generate_vjp(g, (bins, vals), xi, gv, gl)
+    for dt, tol_x, tol_v in ((torch.float64, 1e-8, 1e-8), (torch.float32, 1e-4, 1e-3)):
+        gx, gvals = gc.generate_vjp(_t(g.points, cuda_device, dt), _t(g.indices, cuda_device),
+                                    _t(g.neighbors, cuda_device), g.offsets, _t(bins, cuda_device, dt),
+                                    _t(vals, cuda_device, dt), _t(xi, cuda_device, dt), _t(gv, cuda_device, dt), gl)
+        st = gc.last_status()
+        assert st["error"] == 0 and st["timeouts"] == 0, st
+        assert rel_err(gx.cpu().numpy(), rx) < tol_x, dt
+        assert rel_err(gvals.cpu().numpy(), rv) < tol_v, dt
