@@ -208,9 +208,17 @@ static cudaError_t launch_knn_d(const PointSource<T, D>& src, long long n, int k
   if (k > 32) {
     (ggp::count_launch(), knn_kernel_wide<T, D><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
   } else if (idx32) {
-    if (k <= 8) (ggp::count_launch(), knn_kernel<T, D, 8, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
-    else if (k <= 16) (ggp::count_launch(), knn_kernel<T, D, 16, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
-    else (ggp::count_launch(), knn_kernel<T, D, 32, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+    if (k <= 8) {
+      (ggp::count_launch(), knn_kernel<T, D, 8, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
+    } else if (k <= 16) {
+      constexpr size_t smem = 16 * 128 * KnnHeapSmem<T>::bytes_per_entry;
+      (ggp::count_launch(), knn_heap_kernel<T, D, 16, int><<<grid, 128, smem, s>>>(src, n, k, q, m, nq, q0, out));
+    } else {
+      constexpr size_t smem = 32 * 128 * KnnHeapSmem<T>::bytes_per_entry;
+      auto kern = knn_heap_kernel<T, D, 32, int>;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(src, n, k, q, m, nq, q0, out));
+    }
   } else {
     if (k <= 8) (ggp::count_launch(), knn_kernel<T, D, 8, long long><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
     else if (k <= 16) (ggp::count_launch(), knn_kernel<T, D, 16, long long><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));

@@ -199,6 +199,138 @@ __global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long lo
   }
 }
 
+// The same traversal with the k slots kept as a max-heap in shared memory (k <= KMAX <= 32). The heap is
+// ordered by (squared distance, then lower slot index first), so its top is exactly "the first slot holding
+// the largest squared distance" that the reference replaces (tree.py:84-91); a replacement puts the new point
+// into that slot and sifts it down (log k steps instead of rewriting and rescanning every slot), and the
+// final set is the same. Entry e of thread t lives at [e * blockDim + t]: conflict-free banks whatever entry
+// each thread touches.
+template <typename T> struct KnnHeapSmem {
+  static constexpr size_t bytes_per_entry = sizeof(T) + sizeof(int) + 1;
+};
+
+template <typename T, int D, int KMAX, typename IDX>
+__global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, long long n, int k,
+                                                       const int* __restrict__ query_idx,
+                                                       const int* __restrict__ max_idx, long long nq, long long q0,
+                                                       int* __restrict__ out) {
+  constexpr int PD = D > 0 ? D : kKnnMaxD;
+  extern __shared__ __align__(16) unsigned char knn_smem[];
+  const int bd = blockDim.x;
+  T* hd = reinterpret_cast<T*>(knn_smem) + threadIdx.x;
+  int* hi = reinterpret_cast<int*>(knn_smem + sizeof(T) * KMAX * bd) + threadIdx.x;
+  unsigned char* hs = knn_smem + (sizeof(T) + sizeof(int)) * KMAX * bd + threadIdx.x;
+  const T inf = (T)INFINITY;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += (long long)gridDim.x * blockDim.x) {
+    long long qi = query_idx ? (long long)query_idx[t] : q0 + t;
+    qi = qi < 0 ? 0 : (qi >= n ? n - 1 : qi);  // out-of-range query ids clamp like a JAX gather
+    long long mx = max_idx ? (long long)max_idx[t] : qi;
+    if (mx > n) mx = n;
+    T q[PD];
+    int qs;
+    src.load(qi, q, qs);
+    for (int e = 0; e < k; ++e) {
+      hd[e * bd] = inf;
+      hi[e * bd] = -1;
+      hs[e * bd] = (unsigned char)e;
+    }
+    T maxv = inf;
+    const IDX mxi = (IDX)mx;
+    IDX cur = mx > 0 ? 0 : -1, prev = -1;
+    while (cur != -1) {
+      const IDX par = tree_parent(cur);
+      T p[PD];
+      int s;
+      src.load(cur, p, s);
+      if (prev == par) {
+        const T d2 = sqdist<T, D>(q, p, src.d);
+        if (d2 < maxv) {
+          const int ns = hs[0];
+          int i = 0;
+          for (;;) {
+            const int l = 2 * i + 1;
+            if (l >= k) break;
+            int c = l;
+            T cd = hd[l * bd];
+            int cs = hs[l * bd];
+            if (l + 1 < k) {
+              const T rd = hd[(l + 1) * bd];
+              const int rs = hs[(l + 1) * bd];
+              if (rd > cd || (rd == cd && rs < cs)) { c = l + 1; cd = rd; cs = rs; }
+            }
+            if (cd > d2 || (cd == d2 && cs < ns)) {
+              hd[i * bd] = cd;
+              hs[i * bd] = (unsigned char)cs;
+              hi[i * bd] = hi[c * bd];
+              i = c;
+            } else {
+              break;
+            }
+          }
+          hd[i * bd] = d2;
+          hs[i * bd] = (unsigned char)ns;
+          hi[i * bd] = (int)cur;
+          maxv = hd[0];
+        }
+      }
+      const T sd = rn_sub(coord<T, D>(q, s), coord<T, D>(p, s));
+      const int lvl = tree_level((IDX)(cur + 1));
+      const IDX left = cur + ((IDX)1 << lvl), right = cur + ((IDX)2 << lvl);
+      const IDX nearc = sd < T(0) ? left : right;
+      const IDX farc = sd < T(0) ? right : left;
+      const bool far_in = rn_mul(sd, sd) <= maxv;
+      IDX next;
+      if (prev == nearc || (prev == par && nearc >= mxi)) next = (farc < mxi && far_in) ? farc : par;
+      else next = (prev == par) ? nearc : par;
+      prev = cur;
+      cur = next;
+    }
+    // order by (sqrt(d2), index); an unfilled slot (-1) measures against the last point like the
+    // reference's points[-1] gather (tree.py:103)
+    T key[KMAX];
+    int nb[KMAX];
+#pragma unroll
+    for (int j = 0; j < KMAX; ++j) {
+      if (j < k) {
+        T dd = hd[j * bd];
+        nb[j] = hi[j * bd];
+        if (nb[j] < 0) {
+          T p[PD];
+          int s;
+          src.load(n - 1, p, s);
+          dd = sqdist<T, D>(p, q, src.d);
+        }
+        key[j] = rn_sqrt(dd);
+      } else {
+        key[j] = inf;
+        nb[j] = 0x7fffffff;
+      }
+    }
+#pragma unroll
+    for (int size = 2; size <= KMAX; size <<= 1) {
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+        for (int i = 0; i < KMAX; ++i) {
+          const int j = i ^ stride;
+          if (j > i) {
+            const bool j_less = (key[j] < key[i]) || (key[j] == key[i] && nb[j] < nb[i]);
+            const bool sw = ((i & size) == 0) ? j_less : !j_less;
+            if (sw) {
+              const T tk = key[i]; key[i] = key[j]; key[j] = tk;
+              const int ti = nb[i]; nb[i] = nb[j]; nb[j] = ti;
+            }
+          }
+        }
+      }
+    }
+    int* o = out + t * k;
+#pragma unroll
+    for (int j = 0; j < KMAX; ++j)
+      if (j < k) o[j] = nb[j];
+  }
+}
+
 }  // namespace ggp
 
 namespace ggp {
