@@ -285,25 +285,21 @@ __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, lo
       prev = cur;
       cur = next;
     }
-    // order by (sqrt(d2), index); an unfilled slot (-1) measures against the last point like the
-    // reference's points[-1] gather (tree.py:103)
-    T key[KMAX];
-    int nb[KMAX];
-#pragma unroll
+    // order by (sqrt(d2), index) in the heap's own storage (keys replace the squared distances; entries past k
+    // hold (inf, INT_MAX) and sort last)
     for (int j = 0; j < KMAX; ++j) {
       if (j < k) {
         T dd = hd[j * bd];
-        nb[j] = hi[j * bd];
-        if (nb[j] < 0) {
+        if (hi[j * bd] < 0) {
           T p[PD];
           int s;
           src.load(n - 1, p, s);
           dd = sqdist<T, D>(p, q, src.d);
         }
-        key[j] = rn_sqrt(dd);
+        hd[j * bd] = rn_sqrt(dd);
       } else {
-        key[j] = inf;
-        nb[j] = 0x7fffffff;
+        hd[j * bd] = inf;
+        hi[j * bd] = 0x7fffffff;
       }
     }
 #pragma unroll
@@ -314,20 +310,20 @@ __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, lo
         for (int i = 0; i < KMAX; ++i) {
           const int j = i ^ stride;
           if (j > i) {
-            const bool j_less = (key[j] < key[i]) || (key[j] == key[i] && nb[j] < nb[i]);
+            const T ki = hd[i * bd], kj = hd[j * bd];
+            const int ii = hi[i * bd], ij = hi[j * bd];
+            const bool j_less = (kj < ki) || (kj == ki && ij < ii);
             const bool sw = ((i & size) == 0) ? j_less : !j_less;
             if (sw) {
-              const T tk = key[i]; key[i] = key[j]; key[j] = tk;
-              const int ti = nb[i]; nb[i] = nb[j]; nb[j] = ti;
+              hd[i * bd] = kj; hd[j * bd] = ki;
+              hi[i * bd] = ij; hi[j * bd] = ii;
             }
           }
         }
       }
     }
     int* o = out + t * k;
-#pragma unroll
-    for (int j = 0; j < KMAX; ++j)
-      if (j < k) o[j] = nb[j];
+    for (int j = 0; j < k; ++j) o[j] = hi[j * bd];
   }
 }
 
