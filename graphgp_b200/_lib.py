@@ -92,10 +92,10 @@ _SIGS = {
     "ggp_generate_inv_f64": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _SZ, _P], _I),
     "ggp_generate_logdet_f32": ([_P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _D, _P, _SZ, _P], _I),
     "ggp_generate_logdet_f64": ([_P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _SZ, _P], _I),
-    "ggp_generate_vjp_f32": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _D, _P, _P, _D, _P, _SZ,
+    "ggp_generate_vjp_f32": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _D, _P, _P, _D, _P,
+                              _SZ, _P], _I),
+    "ggp_generate_vjp_f64": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _D, _P, _P, _P, _SZ,
                               _P], _I),
-    "ggp_generate_vjp_f64": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _D, _P, _P, _P, _SZ, _P],
-                             _I),
     "ggp_wait_probe": ([_U64, C.POINTER(C.c_int), _P, _SZ, _P], _I),
 }
 

@@ -558,8 +558,8 @@ cudaError_t vjp_quad_dispatch_k(const VjpParams<T>& v, int k, int max_blocks, cu
 template <typename T>
 int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                         const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* xi,
-                        const T* g_values, double g_logdet, T* out_grad_xi, double* out_grad_vals, double tau,
-                        void* wsp, size_t ws_bytes, cudaStream_t s) {
+                        const T* values, const T* g_values, double g_logdet, T* out_grad_xi, double* out_grad_vals,
+                        double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
   int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !xi || !g_values || !out_grad_xi || !out_grad_vals) return GGP_ERR_INVALID;
@@ -574,15 +574,21 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
   double* X = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
   double* XT = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
-  // forward recompute: values in graph order (workspace), dense factor L0 kept in ws.dense
+  // forward values in graph order (workspace): the caller's generate output when given (the primal output that
+  // a custom_vjp keeps as its residual), else recomputed; the dense factor L0 is kept in ws.dense either way
   T* vg = (T*)ws.values_graph;
-  (ggp::count_launch(), init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, nullptr, n0, n, offsets, n_offsets));
-  if ((rc = dense_root<T>(ws, points, n0, d, 0, xi, perm, vg, nullptr, nullptr, s))) return rc;
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
   p.values = vg;
   p.xi = perm ? xi : xi + n0;
   p.perm = perm;
-  if ((rc = run_cond<T>(p, kGenerate, nb, s))) return rc;
+  if (values) {
+    (ggp::count_launch(), gather_kernel<T><<<grid_for(n), 256, 0, s>>>(values, perm, vg, n));
+    if ((rc = dense_root<T>(ws, points, n0, d, 0, xi, perm, vg, nullptr, nullptr, s))) return rc;
+  } else {
+    (ggp::count_launch(), init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, nullptr, n0, n, offsets, n_offsets));
+    if ((rc = dense_root<T>(ws, points, n0, d, 0, xi, perm, vg, nullptr, nullptr, s))) return rc;
+    if ((rc = run_cond<T>(p, kGenerate, nb, s))) return rc;
+  }
   // reverse sweep over the refined points
   (ggp::count_launch(), gather_kernel<T><<<grid_for(n), 256, 0, s>>>(g_values, perm, vbar, n));
   cudaMemsetAsync(partials, 0, sizeof(double) * (size_t)(kVjpMaxGrid + kRootHistGrid) * nb, s);
@@ -633,20 +639,20 @@ extern "C" {
 
 int ggp_generate_vjp_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const float* cov_bins,
-                         const float* cov_vals, int n_bins, const float* xi, const float* g_values, double g_logdet,
-                         float* out_grad_xi, double* out_grad_vals, double tau, void* workspace,
-                         size_t workspace_bytes, ggp_stream_t stream) {
+                         const float* cov_vals, int n_bins, const float* xi, const float* values,
+                         const float* g_values, double g_logdet, float* out_grad_xi, double* out_grad_vals, double tau,
+                         void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
   return generate_vjp_device<float>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
-                                    n_bins, xi, g_values, g_logdet, out_grad_xi, out_grad_vals, tau, workspace,
+                                    n_bins, xi, values, g_values, g_logdet, out_grad_xi, out_grad_vals, tau, workspace,
                                     workspace_bytes, GGP_STREAM(stream));
 }
 int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const double* cov_bins,
-                         const double* cov_vals, int n_bins, const double* xi, const double* g_values, double g_logdet,
-                         double* out_grad_xi, double* out_grad_vals, void* workspace, size_t workspace_bytes,
-                         ggp_stream_t stream) {
+                         const double* cov_vals, int n_bins, const double* xi, const double* values,
+                         const double* g_values, double g_logdet, double* out_grad_xi, double* out_grad_vals,
+                         void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
   return generate_vjp_device<double>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
-                                     n_bins, xi, g_values, g_logdet, out_grad_xi, out_grad_vals, 0.0, workspace,
+                                     n_bins, xi, values, g_values, g_logdet, out_grad_xi, out_grad_vals, 0.0, workspace,
                                      workspace_bytes, GGP_STREAM(stream));
 }
 

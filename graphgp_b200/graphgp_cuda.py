@@ -377,8 +377,11 @@ def generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=DEFAU
 
 
 def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_values, g_logdet=0.0, *,
-                 tau=DEFAULT_TAU):
-    """Adjoint of generate (+ g_logdet * generate_logdet): returns (grad_xi (N,), grad_cov_vals (n_bins,) f64)."""
+                 tau=DEFAULT_TAU, values=None):
+    """Adjoint of generate (+ g_logdet * generate_logdet): returns (grad_xi (N,), grad_cov_vals (n_bins,) f64).
+
+    ``values``: generate's output for these same inputs, if the caller has it (the primal output a custom_vjp
+    keeps); it saves recomputing the forward pass. Per-point factorisations are recomputed either way."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
     xi = _cuda(xi, "xi", points.dtype)
@@ -386,17 +389,23 @@ def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_
     if xi.numel() != n or g.numel() != n:
         raise ValueError("xi and g_values must have one entry per point")
     idx = None if indices is None else _ids(indices, "indices")
+    if values is not None:
+        values = _cuda(values, "values", points.dtype)
+        if values.numel() != n:
+            raise ValueError("values must have one entry per point")
     gx = torch.empty(n, dtype=points.dtype, device=points.device)
     gv = torch.empty(len(bins), dtype=torch.float64, device=points.device)
     ws = _workspace("GENERATE_VJP", n, d, n0, k, len(bins), len(offs), points.element_size(), points.device)
     lib = _lib.load()
     if sfx == "f32":
         rc = lib.ggp_generate_vjp_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
-                                      _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(g), float(g_logdet), _ptr(gx),
+                                      _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(values), _ptr(g),
+                                      float(g_logdet), _ptr(gx),
                                       _ptr(gv), float(tau), _ptr(ws), ws.numel(), _stream())
     else:
         rc = lib.ggp_generate_vjp_f64(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
-                                      _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(g), float(g_logdet), _ptr(gx),
+                                      _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(values), _ptr(g),
+                                      float(g_logdet), _ptr(gx),
                                       _ptr(gv), _ptr(ws), ws.numel(), _stream())
     _lib.check(rc, "generate_vjp")
     return gx, gv

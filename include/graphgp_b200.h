@@ -243,18 +243,21 @@ int ggp_generate_logdet_f64(const double* points, int64_t n, int d, int64_t n0, 
 /* scalar cotangent g_logdet for generate_logdet, writes                                            */
 /*   out_grad_xi (n,)        = d/dxi  <g_values, generate(xi)>                                       */
 /*   out_grad_vals (n_bins,) = d/dcov_vals [<g_values, generate(xi)> + g_logdet * generate_logdet]   */
-/* out_grad_vals is FP64. Per-point Cholesky factors are recomputed, never stored.                   */
+/* out_grad_vals is FP64. Per-point Cholesky factors are recomputed, never stored. `values` is       */
+/* generate's output for the same inputs (caller order), the primal output a custom_vjp keeps as its  */
+/* residual: passing it skips recomputing the forward pass; NULL recomputes it.                     */
 /* ---------------------------------------------------------------------------------------------- */
 int ggp_generate_vjp_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                          const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
-                         const float* g_values, double g_logdet, float* out_grad_xi, double* out_grad_vals,
-                         double tau, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+                         const float* values, const float* g_values, double g_logdet, float* out_grad_xi,
+                         double* out_grad_vals, double tau, void* workspace, size_t workspace_bytes,
+                         ggp_stream_t stream);
 int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                          const double* cov_bins, const double* cov_vals, int n_bins, const double* xi,
-                         const double* g_values, double g_logdet, double* out_grad_xi, double* out_grad_vals,
-                         void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+                         const double* values, const double* g_values, double g_logdet, double* out_grad_xi,
+                         double* out_grad_vals, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
 
 /* ---------------------------------------------------------------------------------------------- */
 /* Failure-detection probe: launches one kernel whose single wait watches a flag that nothing sets,  */

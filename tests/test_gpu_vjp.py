@@ -149,3 +149,24 @@ def test_vjp_general_kernel_vs_oracle(cuda_device, n, d, n0, k, tab, gl):
         assert st["error"] == 0 and st["timeouts"] == 0, st
         assert rel_err(gx.cpu().numpy(), rx) < tol_x, dt
         assert rel_err(gvals.cpu().numpy(), rv) < tol_v, dt
+
+
+@pytest.mark.parametrize("n,d,n0,k,tab,gl", [CASES[1], GENERAL_CASES[0]])
+def test_vjp_with_forward_values_matches_recompute(cuda_device, n, d, n0, k, tab, gl):
+    """Passing generate's output (values=) gives the gradients of the recomputing path: FP64 to 1e-12, FP32 to 1e-6
+    (the cotangent scatter adds in a scheduling-dependent order)."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    pts, g = oracle_graph(n, d, n0, k)
+    bins, vals = _table(tab)
+    rng = np.random.default_rng(n + 11)
+    xi, gv = rng.standard_normal(n), rng.standard_normal(n)
+    for dt, tol in ((torch.float64, 1e-12), (torch.float32, 1e-6)):
+        args = (_t(g.points, cuda_device, dt), _t(g.indices, cuda_device), _t(g.neighbors, cuda_device), g.offsets,
+                _t(bins, cuda_device, dt), _t(vals, cuda_device, dt), _t(xi, cuda_device, dt))
+        v = gc.generate(*args)
+        a_x, a_v = gc.generate_vjp(*args, _t(gv, cuda_device, dt), gl)
+        b_x, b_v = gc.generate_vjp(*args, _t(gv, cuda_device, dt), gl, values=v)
+        assert rel_err(b_x.cpu().numpy(), a_x.cpu().numpy()) < tol, dt
+        assert rel_err(b_v.cpu().numpy(), a_v.cpu().numpy()) < tol, dt
