@@ -706,12 +706,20 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=200000)
     ap.add_argument("--serving-requests", type=int, default=4096, help="0 skips the serving stream")
     ap.add_argument("--largest", action="store_true", help="also run the 2^28-point largest instance")
+    ap.add_argument("--only-differentiation", action="store_true",
+                    help="run only the differentiation workload and print its object")
     ap.add_argument("--largest-n", type=int, default=1 << 28)
     ap.add_argument("--fd-directions", type=int, default=64,
                     help="finite-difference directions of the differentiation workload (0 skips it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
+    if args.only_differentiation:
+        import torch
+
+        torch.cuda.set_device(local)
+        print(json.dumps(differentiation(torch.device("cuda", local), n_dirs=args.fd_directions)), flush=True)
+        return
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
