@@ -51,3 +51,20 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(ImportError):
         _lib.load()
+
+
+def test_dataflow_width_knob():
+    """ggp_set_dataflow_width / ggp_get_dataflow_width are host-only (no device needed): negative widths clamp to
+    0 (one full persistent grid), and the default is restored afterwards."""
+    from graphgp_b200 import _lib
+
+    lib = _lib.load()
+    old = lib.ggp_get_dataflow_width()
+    try:
+        lib.ggp_set_dataflow_width(8.0)
+        assert lib.ggp_get_dataflow_width() == 8.0
+        lib.ggp_set_dataflow_width(-3.0)
+        assert lib.ggp_get_dataflow_width() == 0.0
+    finally:
+        lib.ggp_set_dataflow_width(old)
+    assert lib.ggp_get_dataflow_width() == old == 4.0
