@@ -6,4 +6,6 @@
 namespace ggp {
 GGP_INSTANTIATE_FAST(float, 20, 2, false)
 GGP_INSTANTIATE_FAST(float, 20, 3, false)
+GGP_INSTANTIATE_FAST(float, 20, 2, true)
+GGP_INSTANTIATE_FAST(float, 20, 3, true)
 }  // namespace ggp

@@ -8,4 +8,6 @@ GGP_INSTANTIATE_FAST(float, 8, 2, false)
 GGP_INSTANTIATE_FAST(float, 8, 3, false)
 GGP_INSTANTIATE_FAST(float, 10, 2, false)
 GGP_INSTANTIATE_FAST(float, 10, 3, false)
+GGP_INSTANTIATE_FAST(float, 8, 2, true)
+GGP_INSTANTIATE_FAST(float, 8, 3, true)
 }  // namespace ggp

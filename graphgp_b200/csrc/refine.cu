@@ -120,12 +120,16 @@ cudaError_t dispatch_k(const RefineParams<T>& p, int kind, int nb, int max_block
     case 20: return launch_fast<T, 20, D, false>(p, kind, nb, max_blocks, s);
     default: break;
   }
+  // other k: the next instantiated size with padding slots (inert rows and columns)
   if constexpr (sizeof(T) == 4) {
     if (k == 32) return launch_fast<T, 32, D, false>(p, kind, nb, max_blocks, s);
+    if (k < 8) return launch_fast<T, 8, D, true>(p, kind, nb, max_blocks, s);
     if (k < 16) return launch_fast<T, 16, D, true>(p, kind, nb, max_blocks, s);
+    if (k < 20) return launch_fast<T, 20, D, true>(p, kind, nb, max_blocks, s);
     if (k < 32) return launch_fast<T, 32, D, true>(p, kind, nb, max_blocks, s);
   } else {
     if (k < 16) return launch_fast<T, 16, D, true>(p, kind, nb, max_blocks, s);
+    if (k < 20) return launch_fast<T, 20, D, true>(p, kind, nb, max_blocks, s);
   }
   return launch_generic<T>(p, kind, max_blocks, s);
 }

@@ -25,8 +25,9 @@ CASES = [  # (n, d, n0, k, table)
     (3000, 3, 128, 8, "rbf"),
     (3000, 2, 128, 20, "rbf"),
     (3000, 3, 128, 32, "rbf"),
-    (3000, 2, 128, 5, "rbf"),     # padded to 16
+    (3000, 2, 128, 5, "rbf"),     # padded to 8 (FP32), 16 (FP64)
     (3000, 3, 128, 12, "matern"),  # padded to 16
+    (2500, 2, 128, 18, "matern"),  # padded to 20
     (2000, 3, 128, 24, "rbf"),     # padded to 32
 ]
 
@@ -74,7 +75,7 @@ def test_refine_f32_vs_oracle(cuda_device, n, d, n0, k, tab):
     assert abs(float(ld) - rld) / abs(rld) < TOL32
 
 
-@pytest.mark.parametrize("n,d,n0,k,tab", [c for c in CASES if c[3] in (8, 10, 16, 20, 5, 12)])
+@pytest.mark.parametrize("n,d,n0,k,tab", [c for c in CASES if c[3] in (8, 10, 16, 20, 5, 12, 18)])
 def test_refine_f64_vs_oracle(cuda_device, n, d, n0, k, tab):
     from graphgp_b200 import graphgp_cuda as gc
 
