@@ -411,6 +411,50 @@ def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_
     return gx, gv
 
 
+_REQUEST_OPS = {"generate": 0, "inverse": 1, "logdet": 2}
+
+
+def request(op, points, n0, k, cov_bins, cov_vals, payload=None, *, tau=DEFAULT_TAU):
+    """Graph build plus one operation in a single native call (``ggp_request_*``): op "generate" (payload = xi)
+    or "inverse" (payload = values) -> (N,) tensor in the caller's order; "logdet" -> 0-d float64 tensor. Builds
+    the same graph as ``build_graph(points, n0=n0, k=k)``; the call waits on the current stream once."""
+    if op not in _REQUEST_OPS:
+        raise ValueError(f"unknown op {op!r}")
+    if n0 < k:
+        raise ValueError(f"n0 must be at least k. Got n0={n0}, k={k}.")
+    points = _cuda(points, "points")
+    if points.ndim != 2:
+        raise ValueError(f"Points must have shape (N, d). Got shape {tuple(points.shape)}.")
+    sfx = _suffix(points.dtype)
+    n, d = points.shape
+    if n0 > n:
+        raise ValueError("n0 must not exceed the number of points")
+    bins, vals = _table(cov_bins, cov_vals, points.dtype)
+    m = _REQUEST_OPS[op]
+    lib = _lib.load()
+    out = ld = None
+    if m < 2:
+        payload = _cuda(payload, "payload", points.dtype)
+        if payload.numel() != n:
+            raise ValueError("payload must have one entry per point")
+        out = torch.empty(n, dtype=points.dtype, device=points.device)
+    else:
+        ld = torch.empty((), dtype=torch.float64, device=points.device)
+    size = lib.ggp_request_buffer_size(m, n, d, int(n0), int(k), len(bins), points.element_size())
+    buf = torch.empty(max(size, 256), dtype=torch.uint8, device=points.device)
+    _tls.last_ws = buf
+    if sfx == "f32":
+        rc = lib.ggp_request_f32(m, _ptr(points), n, d, int(n0), int(k), _ptr(bins), _ptr(vals), len(bins),
+                                 _ptr(payload if m < 2 else None), _ptr(out), _ptr(ld), float(tau), _ptr(buf),
+                                 buf.numel(), _stream())
+    else:
+        rc = lib.ggp_request_f64(m, _ptr(points), n, d, int(n0), int(k), _ptr(bins), _ptr(vals), len(bins),
+                                 _ptr(payload if m < 2 else None), _ptr(out), _ptr(ld), _ptr(buf), buf.numel(),
+                                 _stream())
+    _lib.check(rc, "request")
+    return out if m < 2 else ld
+
+
 def wait_probe(timeout_ns=1_000_000):
     """Run the bounded-wait probe kernel; returns the status code it observed (GGP_ERR_TIMEOUT expected)."""
     dev = torch.device("cuda", torch.cuda.current_device())

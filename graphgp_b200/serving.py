@@ -242,6 +242,16 @@ class Engine:
                 return (torch.as_tensor(np.asarray(req.bins), dtype=self.dtype).to(dev, non_blocking=True),
                         torch.as_tensor(np.asarray(req.vals), dtype=self.dtype).to(dev, non_blocking=True))
 
+            if req.graph_key is None and req.table_key is None:
+                # nothing resident to reuse: graph build and operation in one native call
+                P = torch.from_numpy(np.ascontiguousarray(req.points, self._np)).to(dev, non_blocking=True)
+                B, V = make_table()
+                x = None
+                if req.op in ("generate", "inverse"):
+                    x = torch.from_numpy(np.ascontiguousarray(req.payload, self._np)).to(dev, non_blocking=True)
+                r = gc.request(req.op, P, req.n0, req.k, B, V, x, tau=self.tau)
+                out = float(r.item()) if req.op == "logdet" else r.cpu().numpy()
+                return out, gc.last_status()
             gp, gi, gn, _, offs = self._cached(self._graphs, req.graph_key, make_graph)
             B, V = self._cached(self._tables, req.table_key, make_table)
             if req.op in ("generate", "inverse"):

@@ -260,6 +260,26 @@ int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n
                          double* out_grad_vals, void* workspace, size_t workspace_bytes, ggp_stream_t stream);
 
 /* ---------------------------------------------------------------------------------------------- */
+/* One serving request in one call (no counterpart in the reference, which has no request loop):     */
+/* build the graph of `points` (n, d), caller order, then run `op` on it. GGP_REQUEST_GENERATE takes  */
+/* xi in `payload` and writes values to `out_values`; GGP_REQUEST_INVERSE takes values and writes xi  */
+/* (both caller order, n entries); GGP_REQUEST_LOGDET writes the FP64 log-determinant to            */
+/* `out_logdet` (device). `buffer` (256-byte aligned, ggp_request_buffer_size bytes) holds the        */
+/* operation's workspace first, so ggp_read_status(buffer, ...) reads the call's status block, then  */
+/* the graph. The call waits on `stream` once, for the number of depth batches (a host value the     */
+/* operation needs); everything else is enqueued. Returns 0 from the size function for bad          */
+/* arguments.                                                                                        */
+/* ---------------------------------------------------------------------------------------------- */
+enum { GGP_REQUEST_GENERATE = 0, GGP_REQUEST_INVERSE = 1, GGP_REQUEST_LOGDET = 2 };
+size_t ggp_request_buffer_size(int op, int64_t n, int d, int64_t n0, int k, int n_bins, int dtype_bytes);
+int ggp_request_f32(int op, const float* points, int64_t n, int d, int64_t n0, int k, const float* cov_bins,
+                    const float* cov_vals, int n_bins, const float* payload, float* out_values, double* out_logdet,
+                    double tau, void* buffer, size_t buffer_bytes, ggp_stream_t stream);
+int ggp_request_f64(int op, const double* points, int64_t n, int d, int64_t n0, int k, const double* cov_bins,
+                    const double* cov_vals, int n_bins, const double* payload, double* out_values,
+                    double* out_logdet, void* buffer, size_t buffer_bytes, ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
 /* Failure-detection probe: launches one kernel whose single wait watches a flag that nothing sets,  */
 /* bounded by timeout_ns; returns GGP_ERR_TIMEOUT in *out_code (host int) when the bound worked.      */
 /* Synchronises `stream`. No counterpart in the reference (its only device failure signal is NaN).  */

@@ -113,3 +113,28 @@ def test_requests_match_oracle_f64(cuda_device):
     reqs, graphs = _oracle_requests(np.float64)
     res, _ = sv.Engine(cuda_device, slots=4, dtype=torch.float64).run(reqs, realtime=False)
     _check_vs_oracle(reqs, graphs, res, 1e-8, 1e-8)
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_native_request_equals_separate_calls(cuda_device, dtype):
+    """ggp_request_* (graph build + operation in one call) gives exactly what build_graph followed by
+    generate / generate_inv / generate_logdet gives."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    dt = getattr(torch, dtype)
+    r = _stream(1, seed=21, median_n=5000)[0]
+    P = torch.as_tensor(r.points, device=cuda_device).to(dt)
+    B = torch.as_tensor(r.bins, device=cuda_device).to(dt)
+    V = torch.as_tensor(r.vals, device=cuda_device).to(dt)
+    x = torch.as_tensor(np.random.default_rng(0).standard_normal(r.n), device=cuda_device).to(dt)
+    gp, gi, gn, _, offs = gc.build_graph(P, n0=r.n0, k=r.k, return_offsets=True)
+    ref = {"generate": gc.generate(gp, gi, gn, offs, B, V, x), "inverse": gc.generate_inv(gp, gi, gn, offs, B, V, x),
+           "logdet": gc.generate_logdet(gp, gn, offs, B, V)}
+    for op in ("generate", "inverse", "logdet"):
+        out = gc.request(op, P, r.n0, r.k, B, V, None if op == "logdet" else x)
+        assert gc.last_status()["error"] == 0
+        if op == "logdet":
+            assert abs(float(out) - float(ref[op])) <= 1e-12 * abs(float(ref[op]))
+        else:
+            assert torch.equal(out, ref[op]), op
