@@ -540,12 +540,12 @@ def largest(dev, n=1 << 28, steps=2):
 
 def serving(dev, n_requests):
     """The request stream (Poisson arrivals at 2000 req/s, uneven N, d, k, op mix 70/20/10) through the serving
-    engine: 16 slots (one CUDA stream each), 64 GiB admission budget, latency = completion - arrival."""
+    engine: 32 slots (one CUDA stream each), 64 GiB admission budget, latency = completion - arrival."""
     import torch
 
     from graphgp_b200 import serving as sv
 
-    eng = sv.Engine(dev, slots=16, hbm_budget=64 << 30)
+    eng = sv.Engine(dev, slots=32, hbm_budget=64 << 30)
     eng.run(sv.synthetic_stream(n_requests=48, seed=1, median_n=20000), realtime=False)  # warm-up
     t = time.perf_counter()
     reqs = sv.synthetic_stream(n_requests=n_requests, rate=2000.0, seed=0)

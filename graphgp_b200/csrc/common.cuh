@@ -2,6 +2,11 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <mutex>
+#include <set>
+#include <unordered_map>
+#include <utility>
 #include <stdint.h>
 
 #include "../../include/graphgp_b200.h"
@@ -116,17 +121,77 @@ __device__ __forceinline__ unsigned int warp_ticket(unsigned int* counter) {
 // Process-wide width of the dependency-ordered launches (ggp_set_dataflow_width); 0 = full persistent grid.
 double dataflow_width();
 
-// Occupancy-safe persistent grid size for a kernel.
+// Bytes kept free below the per-block shared-memory maximum for a kernel's static shared memory.
+constexpr int kSmemHeadroom = 1024;
+
+// Occupancy-safe persistent grid size for a kernel. The occupancy query is cached per host thread and
+// (kernel, device, block, shared memory): launches repeat with the same shapes, and the query is a driver call.
+struct OccupancyKey {
+  const void* fn;
+  int dev, block;
+  size_t smem;
+  bool operator==(const OccupancyKey& o) const {
+    return fn == o.fn && dev == o.dev && block == o.block && smem == o.smem;
+  }
+};
+struct OccupancyKeyHash {
+  size_t operator()(const OccupancyKey& k) const {
+    return std::hash<const void*>()(k.fn) ^ (std::hash<size_t>()(k.smem) * 31u) ^ ((size_t)k.block << 20) ^
+           ((size_t)k.dev << 40);
+  }
+};
+
 template <typename Kernel>
 inline int persistent_grid(Kernel k, int block, size_t smem, int max_blocks) {
-  int dev = 0, sms = 0, per_sm = 0;
+  thread_local std::unordered_map<OccupancyKey, long, OccupancyKeyHash> cache;
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
-  long g = (long)sms * per_sm;
+  const OccupancyKey key{reinterpret_cast<const void*>(k), dev, block, smem};
+  long g;
+  auto it = cache.find(key);
+  if (it != cache.end()) {
+    g = it->second;
+  } else {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+    g = (long)sms * per_sm;
+    cache.emplace(key, g);
+  }
   if (max_blocks > 0 && g > max_blocks) g = max_blocks;
   if (g < 1) g = 1;
   return (int)g;
+}
+
+// Let `k` use up to `smem` bytes of dynamic shared memory. The limit is raised once per (kernel, device), to
+// the device's opt-in maximum less the kernel's static shared memory, so that host threads launching the same
+// kernel with different sizes never lower it under one another. Launchers size their blocks to fit
+// kSmemHeadroom below the opt-in maximum, which covers every kernel's static shared memory.
+template <typename Kernel>
+inline cudaError_t allow_smem(Kernel k, size_t smem) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  thread_local std::set<std::pair<const void*, int>> seen;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(k), dev);
+  if (seen.count(key)) return cudaSuccess;
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done.count(key)) {
+    int optin = 0;
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
+    // the limit covers dynamic shared memory only; the kernel's static shared memory counts against the same
+    // per-block maximum
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    if (e != cudaSuccess) return e;
+    done.insert(key);
+  }
+  seen.insert(key);
+  return cudaSuccess;
 }
 
 }  // namespace ggp

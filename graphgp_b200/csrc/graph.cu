@@ -216,7 +216,7 @@ static cudaError_t launch_knn_d(const PointSource<T, D>& src, long long n, int k
     } else {
       constexpr size_t smem = 32 * 128 * KnnHeapSmem<T>::bytes_per_entry;
       auto kern = knn_heap_kernel<T, D, 32, int>;
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      allow_smem(kern, smem);
       (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(src, n, k, q, m, nq, q0, out));
     }
   } else {

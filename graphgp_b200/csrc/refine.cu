@@ -613,7 +613,7 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
   if (!swept && n > n0 && n_offsets > 1) {
     const size_t smem = v.r.table_smem + sizeof(double) * (size_t)nb;
     auto kern = vjp_refine_kernel<T>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_smem(kern, smem);
     if (e != cudaSuccess) return cuda_status(e);
     const int cap = dataflow_blocks(n, n0, n_offsets - 1, 4);
     const int grid = persistent_grid(kern, 128, smem, cap > 0 && cap < kVjpMaxGrid ? cap : kVjpMaxGrid);
@@ -629,7 +629,7 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
   (ggp::count_launch(), transpose_kernel<<<grid_for(n0 * n0), 256, 0, s>>>(X, n0, XT));
   (ggp::count_launch(), row_solve_kernel<<<grid_for(n0 * 32), 256, 0, s>>>(XT, LT, n0, 0));
   const size_t hsmem = sizeof(double) * (size_t)nb;
-  cudaFuncSetAttribute(root_hist_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  allow_smem(root_hist_kernel<T>, hsmem);
   (ggp::count_launch(), root_hist_kernel<T><<<kRootHistGrid, 256, hsmem, s>>>(XT, points, n0, d, ws.table, nb,
                                                                                partials + (size_t)kVjpMaxGrid * nb));
   (ggp::count_launch(), reduce_columns_kernel<<<(nb + 255) / 256, 256, 0, s>>>(partials, kVjpMaxGrid + kRootHistGrid, nb,

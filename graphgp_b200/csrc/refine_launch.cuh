@@ -26,13 +26,13 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     // as many warps (up to the launch bound) as the shared memory left by the table holds
     const size_t per_warp = sizeof(T) * 8 * QuadSmem<K, D>::kPerPoint;
-    long warps = ((long)optin - q.table_smem) / (long)per_warp;
+    long warps = ((long)optin - kSmemHeadroom - q.table_smem) / (long)per_warp;
     if (warps > Quad2Block<T>::kMax / 32) warps = Quad2Block<T>::kMax / 32;
     if (warps < 1) return launch_generic<T>(p, kind, max_blocks < 0 ? 0 : max_blocks, s);
     const int block = (int)warps * 32;
     const size_t smem = q.table_smem + per_warp * warps;
     auto kern = (kind == kCond) ? refine_quad2_kernel<T, K, D, PAD, false> : refine_quad2_kernel<T, K, D, PAD, true>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_smem(kern, smem);
     if (e != cudaSuccess) return e;
     if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, block / 32);
     int grid = persistent_grid(kern, block, smem, 0);
@@ -44,12 +44,12 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
   if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, 4);
   if (kind == kCond) {
     auto kern = refine_quad_kernel<T, K, D, PAD, false>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_smem(kern, smem);
     const int grid = persistent_grid(kern, 128, smem, max_blocks);
     (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));
   } else {
     auto kern = refine_quad_kernel<T, K, D, PAD, true>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_smem(kern, smem);
     const int grid = persistent_grid(kern, 128, smem, max_blocks);
     (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));
   }
@@ -61,7 +61,7 @@ cudaError_t launch_generic(const RefineParams<T>& p, int kind, int max_blocks, c
   if (max_blocks < 0) max_blocks = 0;
   const size_t smem = generic_smem_bytes(p.k, p.d);
   auto kern = refine_generic_kernel<T>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int grid = persistent_grid(kern, 128, smem, max_blocks);
   const int mode = (kind == kLogdet) ? 2 : p.mode;

@@ -310,11 +310,12 @@ cudaError_t launch_vjp_quad(const VjpParams<T>& v, int max_blocks, cudaStream_t 
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   // the largest block (warps share the staged table) whose shared memory fits
   int block = kMaxBlock;
-  while (block > 32 && vjp_quad_smem<T, K, D>(v.r.table_smem, v.nb, block) > (size_t)optin) block >>= 1;
+  const size_t avail = (size_t)(optin - kSmemHeadroom);
+  while (block > 32 && vjp_quad_smem<T, K, D>(v.r.table_smem, v.nb, block) > avail) block >>= 1;
   const size_t smem = vjp_quad_smem<T, K, D>(v.r.table_smem, v.nb, block);
-  if (smem > (size_t)optin) return cudaErrorInvalidConfiguration;  // the caller takes the one-thread kernel
+  if (smem > avail) return cudaErrorInvalidConfiguration;  // the caller takes the one-thread kernel
   auto kern = vjp_quad_kernel<T, K, D, PAD, kMaxBlock>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int cap = dataflow_blocks(v.r.n, v.r.n0, v.r.n_batches, block / 32);
   if (cap > 0 && (max_blocks <= 0 || cap < max_blocks)) max_blocks = cap;
