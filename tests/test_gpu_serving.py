@@ -138,3 +138,22 @@ def test_native_request_equals_separate_calls(cuda_device, dtype):
             assert abs(float(out) - float(ref[op])) <= 1e-12 * abs(float(ref[op]))
         else:
             assert torch.equal(out, ref[op]), op
+
+
+def test_concurrent_requests_with_different_table_sizes(cuda_device):
+    """Requests whose kernel tables differ in size (so their launches need different shared memory) run on 8
+    streams at once, and each still gives the result it gives alone."""
+    base = _stream(24, seed=31, median_n=4000, n_max=20000)
+    reqs = []
+    for i, r in enumerate(base):
+        nb = (1000, 4097, 257)[i % 3]
+        from graphgp_b200 import extras
+
+        bins, vals = extras.rbf_kernel(variance=1.0, scale=0.2, r_min=1e-4, r_max=10.0, n_bins=nb, jitter=1e-4)
+        reqs.append(sv.Request(r.rid, r.op, r.points, r.k, r.n0, bins, vals, r.payload, 0.0))
+    res, _ = sv.Engine(cuda_device, slots=8).run(reqs, realtime=False)
+    alone = sv.Engine(cuda_device, slots=1)
+    for r, m in zip(reqs, res):
+        out, st = alone.process(r)
+        assert m.status["error"] == 0 and st["error"] == 0
+        assert _same(m.output, out, r.op), (r.rid, len(r.bins))
