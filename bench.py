@@ -546,7 +546,9 @@ def serving(dev, n_requests):
     from graphgp_b200 import serving as sv
 
     eng = sv.Engine(dev, slots=32, hbm_budget=64 << 30)
-    eng.run(sv.synthetic_stream(n_requests=48, seed=1, median_n=20000), realtime=False)  # warm-up
+    # warm-up: one untimed pass over a different stream of the same distribution, so that the device memory
+    # pool has grown to the stream's working set before the timed pass (a running server's steady state)
+    eng.run(sv.synthetic_stream(n_requests=n_requests, rate=2000.0, seed=1), realtime=False)
     t = time.perf_counter()
     reqs = sv.synthetic_stream(n_requests=n_requests, rate=2000.0, seed=0)
     gen_s = time.perf_counter() - t
@@ -554,7 +556,8 @@ def serving(dev, n_requests):
     res, summ = eng.run(reqs, realtime=True)
     bad = sum(1 for r in res if r.status and r.status.get("error"))
     pts = np.array([r.n for r in reqs])
-    summ.update(workload="4096 requests, Poisson 2000 req/s, N lognormal(median 30000, log-sd 1) clipped to "
+    summ.update(warmup="one untimed pass over a 4096-request stream of the same distribution (seed 1)",
+                workload="4096 requests, Poisson 2000 req/s, N lognormal(median 30000, log-sd 1) clipped to "
                          "[1e3, 1e6], d in {2,3}, k in {8,16,32}, n0 = max(k, min(256, N // 100)), RBF table per "
                          "request (scale U(0.05,0.5), r=0 + 999 log bins on [1e-4, 10]); op mix 70/20/10"
                 if n_requests == 4096 else f"{n_requests} requests of the same distribution",

@@ -190,7 +190,7 @@ class Engine:
     (``Request.table_key``) named by a key stay resident on the device for later requests."""
 
     def __init__(self, device=None, slots: int = 16, hbm_budget: int = 32 << 30, tau: Optional[float] = None,
-                 dtype=None):
+                 dtype=None, fused: bool = True):
         import torch
 
         from . import graphgp_cuda as gc
@@ -203,6 +203,7 @@ class Engine:
         self.slots = int(slots)
         self.budget = int(hbm_budget)
         self.tau = gc.DEFAULT_TAU if tau is None else tau
+        self.fused = fused  # requests with nothing resident: one native call (ggp_request_*) or separate calls
         self.dtype = dtype or torch.float32
         if self.dtype not in (torch.float32, torch.float64):
             raise TypeError("dtype must be torch.float32 or torch.float64")
@@ -242,7 +243,7 @@ class Engine:
                 return (torch.as_tensor(np.asarray(req.bins), dtype=self.dtype).to(dev, non_blocking=True),
                         torch.as_tensor(np.asarray(req.vals), dtype=self.dtype).to(dev, non_blocking=True))
 
-            if req.graph_key is None and req.table_key is None:
+            if self.fused and req.graph_key is None and req.table_key is None:
                 # nothing resident to reuse: graph build and operation in one native call
                 P = torch.from_numpy(np.ascontiguousarray(req.points, self._np)).to(dev, non_blocking=True)
                 B, V = make_table()
