@@ -83,25 +83,37 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t
 }
 
 // Exclusive scan of `m` counters in one block (digit-major order gives each (digit, tile) its base).
+// In-place exclusive scan of m counts by one block of 1024 threads, 1024 consecutive entries per step (coalesced):
+// a warp-shuffle scan per warp, a scan of the 32 warp totals, and a running carry between steps.
 __global__ void __launch_bounds__(1024) exclusive_scan_kernel(unsigned int* __restrict__ a, long long m) {
-  __shared__ unsigned long long s[1024];
-  const long long per = (m + blockDim.x - 1) / blockDim.x;
-  const long long lo = threadIdx.x * per, hi = min(m, lo + per);
-  unsigned long long local = 0;
-  for (long long i = lo; i < hi; ++i) local += a[i];
-  s[threadIdx.x] = local;
-  __syncthreads();
-  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-    const unsigned long long v = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+  __shared__ unsigned long long warp_sums[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned long long carry = 0;
+  for (long long base = 0; base < m; base += 1024) {
+    const long long i = base + threadIdx.x;
+    const unsigned long long x = i < m ? a[i] : 0ull;
+    unsigned long long v = x;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    if (lane == 31) warp_sums[wid] = v;
     __syncthreads();
-    s[threadIdx.x] += v;
+    if (wid == 0) {
+      unsigned long long w = warp_sums[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      warp_sums[lane] = w;
+    }
     __syncthreads();
-  }
-  unsigned long long run = s[threadIdx.x] - local;
-  for (long long i = lo; i < hi; ++i) {
-    const unsigned int c = a[i];
-    a[i] = (unsigned int)run;
-    run += c;
+    const unsigned long long before = wid > 0 ? warp_sums[wid - 1] : 0ull;
+    if (i < m) a[i] = (unsigned int)(carry + before + v - x);
+    carry += warp_sums[31];
+    __syncthreads();  // warp_sums is rewritten in the next step
   }
 }
 
