@@ -595,17 +595,23 @@ __global__ void __launch_bounds__(256) tree_leaf_kernel(Level L, int d, long lon
     ix = idx_in[start + lane];
   }
   for (int level = L.level; __any_sync(0xffffffffu, active); ++level) {
+    // the lanes of my node (a finished or idle lane forms a group of its own)
+    const long long node_key = active ? node : -1ll - lane;
+    const unsigned int grp = __match_any_sync(0xffffffffu, node_key);
     // bounding box of my node -> split dim (first argmax of the range)
     int split = 0;
     T bestr = T(0);
     for (int k = 0; k < d; ++k) {
-      U mn = ~(U)0, mx = 0;
       const U mine = order_key(c[k]);
-      for (int src = 0; src < 32; ++src) {
-        const long long nd = __shfl_sync(0xffffffffu, node, src);
-        const bool act = __shfl_sync(0xffffffffu, active, src);
-        const U kk = __shfl_sync(0xffffffffu, mine, src);
-        if (active && act && nd == node) {
+      U mn, mx;
+      if constexpr (sizeof(U) == 4) {
+        mn = __reduce_min_sync(grp, mine);
+        mx = __reduce_max_sync(grp, mine);
+      } else {
+        mn = ~(U)0;
+        mx = 0;
+        for (unsigned int m = grp; m; m &= m - 1) {
+          const U kk = __shfl_sync(grp, mine, __ffs(m) - 1);
           mn = kk < mn ? kk : mn;
           mx = kk > mx ? kk : mx;
         }
@@ -614,18 +620,14 @@ __global__ void __launch_bounds__(256) tree_leaf_kernel(Level L, int d, long lon
       if (k == 0 || r > bestr) { bestr = r; split = k; }
     }
     // rank of my point inside my node under the composite order
-    int rank = 0, size_node = 0;
-    for (int src = 0; src < 32; ++src) {
-      const long long nd = __shfl_sync(0xffffffffu, node, src);
-      const bool act = __shfl_sync(0xffffffffu, active, src);
-      const int oix = __shfl_sync(0xffffffffu, ix, src);
+    int rank = 0;
+    const int size_node = __popc(grp);
+    for (unsigned int m = grp; m; m &= m - 1) {
+      const int src = __ffs(m) - 1;
+      const int oix = __shfl_sync(grp, ix, src);
       T oc[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) oc[k] = __shfl_sync(0xffffffffu, c[k], src);
-      if (active && act && nd == node) {
-        ++size_node;
-        if (src != lane && leaf_less<T>(oc, oix, c, ix, split, level, node, split_out)) ++rank;
-      }
+      for (int k = 0; k < d; ++k) oc[k] = __shfl_sync(grp, c[k], src);
+      if (src != lane && leaf_less<T>(oc, oix, c, ix, split, level, node, split_out)) ++rank;
     }
     if (active) {
       const int mid = size_node / 2;
