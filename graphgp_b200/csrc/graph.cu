@@ -171,9 +171,12 @@ static int build_tree_device(const T* points, long long n, int d, T* out_points,
       (ggp::count_launch(), tree_bbox_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, d, n, w.soa[cur], w.box));
       (ggp::count_launch(), tree_split_kernel<T><<<g_grid(Lv.n_level), 256, 0, s>>>(Lv, d, w.box, w.st, out_split));
       cudaMemsetAsync(w.hist, 0, sizeof(unsigned int) * (size_t)Lv.n_level * kBins, s);
-      for (int p = 0; p < n_passes<KeyType<T>::BITS>(); ++p) {
-        (ggp::count_launch(), tree_hist_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, n, w.soa[cur], w.st, p, w.hist));
-        (ggp::count_launch(), tree_pick_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, w.st, p, w.hist));
+      for (int stage = 0; stage < 2; ++stage) {  // the median, then its ties on the parent's split dim
+        for (int p = 0; p < n_passes<KeyType<T>::BITS>(); ++p) {
+          (ggp::count_launch(), tree_hist_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, n, w.soa[cur], w.idx[cur], w.st,
+                                                                              stage, p, w.hist, out_split));
+          (ggp::count_launch(), tree_pick_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, w.st, stage, p, w.hist));
+        }
       }
       (ggp::count_launch(), tree_tie_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, n, w.soa[cur], w.idx[cur], w.st, out_split));
       cudaMemsetAsync(w.cursor, 0, sizeof(unsigned long long) * (size_t)(2 * Lv.n_level), s);

@@ -298,10 +298,16 @@ __global__ void tree_split_kernel(Level L, int d, const typename KeyType<T>::U* 
   S.n_stages = 0;
 }
 
+// Histogram of one radix digit of the stage key over each node's candidates, several blocks per node. Stage 0:
+// every point, keyed on the node's split dim. Stage 1 (only for nodes whose stage-0 median value is shared by
+// more than one point): the points holding that value, keyed on the parent's split dim (the original index at
+// the root), so that ties at the median resolve with the same block parallelism as the median itself.
 template <typename T>
 __global__ void __launch_bounds__(256) tree_hist_kernel(Level L, int cps, long long n, const T* __restrict__ soa,
-                                                        const SelState<T>* __restrict__ st, int pass,
-                                                        unsigned int* __restrict__ hist) {
+                                                        const int* __restrict__ idx_in,
+                                                        const SelState<T>* __restrict__ st, int stage, int pass,
+                                                        unsigned int* __restrict__ hist,
+                                                        const int* __restrict__ split_out) {
   using U = typename KeyType<T>::U;
   constexpr int BITS = KeyType<T>::BITS;
   __shared__ unsigned int h[kBins];
@@ -310,6 +316,7 @@ __global__ void __launch_bounds__(256) tree_hist_kernel(Level L, int cps, long l
   const long long size = L.seg_size(seg);
   const long long lo = (long long)chunk * kChunkA;
   if (lo >= size) return;
+  if (stage > 0 && st[seg].c_eq <= 1) return;  // the stage-0 median is unique: nothing to resolve
   const long long hi = min(size, lo + kChunkA);
   const long long start = L.seg_start(seg);
   const int shift = BITS - kDigitBits * (pass + 1) > 0 ? BITS - kDigitBits * (pass + 1) : 0;
@@ -317,10 +324,18 @@ __global__ void __launch_bounds__(256) tree_hist_kernel(Level L, int cps, long l
   const U hi_mask = (shift + width >= BITS) ? (U)0 : (~(U)0) << (shift + width);
   const U prefix = st[seg].prefix;
   const int split = st[seg].split;
+  const U sel0 = st[seg].sel[0];
+  // stage-1 key: the parent's split dim (stage_key with stage 1), or the original index at the root
+  const int dim1 = (stage > 0 && L.level >= 1) ? split_out[tree_parent(L.n_above + seg)] : -1;
   for (int b = threadIdx.x; b < kBins; b += blockDim.x) h[b] = 0;
   __syncthreads();
   for (long long e = lo + threadIdx.x; e < hi; e += blockDim.x) {
-    const U k = order_key(soa[(long long)split * n + start + e]);
+    const long long pos = start + e;
+    U k = order_key(soa[(long long)split * n + pos]);
+    if (stage > 0) {
+      if (k != sel0) continue;
+      k = dim1 >= 0 ? order_key(soa[(long long)dim1 * n + pos]) : (U)(uint32_t)idx_in[pos];
+    }
     if ((k & hi_mask) != (prefix & hi_mask)) continue;
     atomicAdd(&h[(int)((k >> shift) & (U)((1u << width) - 1))], 1u);
   }
@@ -331,12 +346,19 @@ __global__ void __launch_bounds__(256) tree_hist_kernel(Level L, int cps, long l
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) tree_pick_kernel(Level L, SelState<T>* st, int pass, unsigned int* hist) {
+__global__ void __launch_bounds__(256) tree_pick_kernel(Level L, SelState<T>* st, int stage, int pass,
+                                                        unsigned int* hist) {
   constexpr int BITS = KeyType<T>::BITS;
   const long long seg = blockIdx.x;
   if (L.seg_size(seg) <= 0) return;
   __shared__ SelState<T> S;
   if (threadIdx.x == 0) S = st[seg];
+  __syncthreads();
+  if (stage > 0 && S.c_eq <= 1) return;  // uniform across the block; its histogram stayed zero
+  if (stage > 0 && pass == 0 && threadIdx.x == 0) {  // a new stage: the rank t carries over
+    S.prefix = 0;
+    S.c_less = 0;
+  }
   __syncthreads();
   const int shift = BITS - kDigitBits * (pass + 1) > 0 ? BITS - kDigitBits * (pass + 1) : 0;
   unsigned int* h = hist + seg * kBins;
@@ -344,25 +366,26 @@ __global__ void __launch_bounds__(256) tree_pick_kernel(Level L, SelState<T>* st
   for (int b = threadIdx.x; b < kBins; b += blockDim.x) h[b] = 0;
   if (threadIdx.x == 0) {
     if (pass == n_passes<BITS>() - 1) {
-      S.sel[0] = S.prefix;
-      S.n_stages = 1;
+      S.sel[stage] = S.prefix;
+      S.n_stages = stage + 1;
     }
     st[seg] = S;
   }
 }
 
-// Ties at the median after stage 0: finish the selection with the later stages (rare).
+// Ties left after stages 0 and 1 (rare: equal coordinates on two split dims): finish the selection with the
+// later stages, one block per node.
 template <typename T>
 __global__ void __launch_bounds__(256) tree_tie_kernel(Level L, long long n, const T* __restrict__ soa,
                                                        const int* __restrict__ idx_in, SelState<T>* st,
                                                        const int* __restrict__ split_out) {
   const long long seg = blockIdx.x;
-  if (L.seg_size(seg) <= 0 || st[seg].c_eq <= 1) return;
+  if (L.seg_size(seg) <= 0 || st[seg].c_eq <= 1 || L.level < 1) return;  // at the root stage 1 is the index
   __shared__ SelState<T> S;
   __shared__ unsigned int h[kBins];
   if (threadIdx.x == 0) S = st[seg];
   __syncthreads();
-  block_select<T>(S, 1, L.level, L.n_above + seg, soa, idx_in, n, L.seg_start(seg), L.seg_size(seg), split_out, h);
+  block_select<T>(S, 2, L.level, L.n_above + seg, soa, idx_in, n, L.seg_start(seg), L.seg_size(seg), split_out, h);
   if (threadIdx.x == 0) st[seg] = S;
 }
 
