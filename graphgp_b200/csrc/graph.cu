@@ -40,6 +40,7 @@ struct TreeWs {
   SelState<T>* st;
   unsigned int* hist;
   unsigned long long* cursor;
+  unsigned int* done;  // per node: blocks of the current selection launch that have finished counting
 };
 
 static long long seg_a_max(long long n) { return n / kSegA + 2; }
@@ -57,7 +58,8 @@ static size_t tree_ws_bytes(long long n, int d, TreeWs<T>* w, char* base) {
   auto* st = (SelState<T>*)c.take(sizeof(SelState<T>) * (size_t)sa);
   auto* hist = (unsigned int*)c.take(sizeof(unsigned int) * (size_t)sa * kBins);
   auto* cur = (unsigned long long*)c.take(sizeof(unsigned long long) * (size_t)(2 * sa + 2));
-  if (w) { w->box = box; w->st = st; w->hist = hist; w->cursor = cur; }
+  auto* done = (unsigned int*)c.take(sizeof(unsigned int) * (size_t)sa);
+  if (w) { w->box = box; w->st = st; w->hist = hist; w->cursor = cur; w->done = done; }
   return c.off;
 }
 
@@ -171,13 +173,11 @@ static int build_tree_device(const T* points, long long n, int d, T* out_points,
       (ggp::count_launch(), tree_bbox_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, d, n, w.soa[cur], w.box));
       (ggp::count_launch(), tree_split_kernel<T><<<g_grid(Lv.n_level), 256, 0, s>>>(Lv, d, w.box, w.st, out_split));
       cudaMemsetAsync(w.hist, 0, sizeof(unsigned int) * (size_t)Lv.n_level * kBins, s);
-      for (int stage = 0; stage < 2; ++stage) {  // the median, then its ties on the parent's split dim
-        for (int p = 0; p < n_passes<KeyType<T>::BITS>(); ++p) {
-          (ggp::count_launch(), tree_hist_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, n, w.soa[cur], w.idx[cur], w.st,
-                                                                              stage, p, w.hist, out_split));
-          (ggp::count_launch(), tree_pick_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, w.st, stage, p, w.hist));
-        }
-      }
+      cudaMemsetAsync(w.done, 0, sizeof(unsigned int) * (size_t)Lv.n_level, s);
+      for (int stage = 0; stage < 2; ++stage)  // the median, then its ties on the parent's split dim
+        for (int p = 0; p < n_passes<KeyType<T>::BITS>(); ++p)
+          (ggp::count_launch(), tree_select_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, cps, n, w.soa[cur], w.idx[cur], w.st, stage,
+                                                                                p, w.hist, w.done, out_split));
       (ggp::count_launch(), tree_tie_kernel<T><<<(unsigned)Lv.n_level, 256, 0, s>>>(Lv, n, w.soa[cur], w.idx[cur], w.st, out_split));
       cudaMemsetAsync(w.cursor, 0, sizeof(unsigned long long) * (size_t)(2 * Lv.n_level), s);
       (ggp::count_launch(), tree_partition_kernel<T><<<(unsigned)grid, 256, 0, s>>>(Lv, N1, cps, d, n, w.soa[cur], w.idx[cur], w.soa[cur ^ 1],

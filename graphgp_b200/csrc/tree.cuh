@@ -298,25 +298,29 @@ __global__ void tree_split_kernel(Level L, int d, const typename KeyType<T>::U* 
   S.n_stages = 0;
 }
 
-// Histogram of one radix digit of the stage key over each node's candidates, several blocks per node. Stage 0:
-// every point, keyed on the node's split dim. Stage 1 (only for nodes whose stage-0 median value is shared by
-// more than one point): the points holding that value, keyed on the parent's split dim (the original index at
-// the root), so that ties at the median resolve with the same block parallelism as the median itself.
+// One radix digit of the median selection, several blocks per node. Each block counts its chunk's candidates
+// into the node's histogram; the node's last block to finish (a completion counter) picks the digit's bin and
+// clears the histogram and the counter for the next launch. Stage 0: every point, keyed on the node's split dim.
+// Stage 1 (only for nodes whose stage-0 median value is shared by more than one point): the points holding that
+// value, keyed on the parent's split dim (the original index at the root), so that ties at the median resolve
+// with the same block parallelism as the median itself.
 template <typename T>
-__global__ void __launch_bounds__(256) tree_hist_kernel(Level L, int cps, long long n, const T* __restrict__ soa,
-                                                        const int* __restrict__ idx_in,
-                                                        const SelState<T>* __restrict__ st, int stage, int pass,
-                                                        unsigned int* __restrict__ hist,
-                                                        const int* __restrict__ split_out) {
+__global__ void __launch_bounds__(256) tree_select_kernel(Level L, int cps, long long n, const T* __restrict__ soa,
+                                                          const int* __restrict__ idx_in, SelState<T>* st,
+                                                          int stage, int pass, unsigned int* __restrict__ hist,
+                                                          unsigned int* __restrict__ done,
+                                                          const int* __restrict__ split_out) {
   using U = typename KeyType<T>::U;
   constexpr int BITS = KeyType<T>::BITS;
   __shared__ unsigned int h[kBins];
+  __shared__ SelState<T> S;
+  __shared__ bool s_last;
   const long long seg = blockIdx.x / cps;
   const int chunk = blockIdx.x % cps;
   const long long size = L.seg_size(seg);
   const long long lo = (long long)chunk * kChunkA;
   if (lo >= size) return;
-  if (stage > 0 && st[seg].c_eq <= 1) return;  // the stage-0 median is unique: nothing to resolve
+  if (stage > 0 && st[seg].c_eq <= 1) return;  // uniform over the node: its stage-0 median is unique
   const long long hi = min(size, lo + kChunkA);
   const long long start = L.seg_start(seg);
   const int shift = BITS - kDigitBits * (pass + 1) > 0 ? BITS - kDigitBits * (pass + 1) : 0;
@@ -343,29 +347,32 @@ __global__ void __launch_bounds__(256) tree_hist_kernel(Level L, int cps, long l
   unsigned int* g = hist + seg * kBins;
   for (int b = threadIdx.x; b < kBins; b += blockDim.x)
     if (h[b]) atomicAdd(&g[b], h[b]);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) tree_pick_kernel(Level L, SelState<T>* st, int stage, int pass,
-                                                        unsigned int* hist) {
-  constexpr int BITS = KeyType<T>::BITS;
-  const long long seg = blockIdx.x;
-  if (L.seg_size(seg) <= 0) return;
-  __shared__ SelState<T> S;
-  if (threadIdx.x == 0) S = st[seg];
+  __threadfence();
   __syncthreads();
-  if (stage > 0 && S.c_eq <= 1) return;  // uniform across the block; its histogram stayed zero
-  if (stage > 0 && pass == 0 && threadIdx.x == 0) {  // a new stage: the rank t carries over
-    S.prefix = 0;
-    S.c_less = 0;
+  if (threadIdx.x == 0) {
+    const unsigned int n_chunks = (unsigned int)((size + kChunkA - 1) / kChunkA);
+    s_last = atomicAdd(&done[seg], 1u) == n_chunks - 1;
   }
   __syncthreads();
-  const int shift = BITS - kDigitBits * (pass + 1) > 0 ? BITS - kDigitBits * (pass + 1) : 0;
-  unsigned int* h = hist + seg * kBins;
-  block_pick_bin<T>(S, h, shift, pass == n_passes<BITS>() - 1);
-  for (int b = threadIdx.x; b < kBins; b += blockDim.x) h[b] = 0;
+  if (!s_last) return;
+  __threadfence();
+  for (int b = threadIdx.x; b < kBins; b += blockDim.x) {
+    h[b] = __ldcg(&g[b]);
+    g[b] = 0;
+  }
   if (threadIdx.x == 0) {
-    if (pass == n_passes<BITS>() - 1) {
+    S = st[seg];
+    done[seg] = 0;
+    if (stage > 0 && pass == 0) {  // a new stage: the rank t carries over
+      S.prefix = 0;
+      S.c_less = 0;
+    }
+  }
+  __syncthreads();
+  const bool last_pass = pass == n_passes<BITS>() - 1;
+  block_pick_bin<T>(S, h, shift, last_pass);
+  if (threadIdx.x == 0) {
+    if (last_pass) {
       S.sel[stage] = S.prefix;
       S.n_stages = stage + 1;
     }
