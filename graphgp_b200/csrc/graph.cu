@@ -1,5 +1,6 @@
 // Graph build host orchestration and C-ABI: k-d tree (tree.cuh), preceding k-NN (knn.cuh), depths and
 // ordering by depth (order.cuh) -- reference graphgp/tree.py and graphgp/graph.py.
+#include <algorithm>
 #include <cstdio>
 
 #include "knn.cuh"
@@ -85,10 +86,12 @@ static size_t order_ws_bytes(long long n, OrderWs* w, char* base) {
 }
 
 template <typename T>
-static size_t knn_ws_bytes(long long n, NodeRec<T>** rec, char* base) {
+static size_t knn_ws_bytes(long long n, NodeRec<T>** rec, char* base, unsigned long long** next_query = nullptr) {
   Carver c(base);
   auto* r = (NodeRec<T>*)c.take(sizeof(NodeRec<T>) * (size_t)n);
+  auto* nq = (unsigned long long*)c.take(sizeof(unsigned long long));
   if (rec) *rec = r;
+  if (next_query) *next_query = nq;
   return c.off;
 }
 
@@ -205,7 +208,8 @@ static int build_tree_device(const T* points, long long n, int d, T* out_points,
 // ------------------------------------------------------------------------------------------------
 template <typename T, int D>
 static cudaError_t launch_knn_d(const PointSource<T, D>& src, long long n, int k, const int* q, const int* m,
-                                long long nq, long long q0, int* out, cudaStream_t s) {
+                                long long nq, long long q0, int* out, unsigned long long* next_query,
+                                cudaStream_t s) {
   const int grid = g_grid(nq, 128);
   const bool idx32 = n < (1ll << 30);  // 32-bit tree indices
   if (k > 32) {
@@ -213,14 +217,21 @@ static cudaError_t launch_knn_d(const PointSource<T, D>& src, long long n, int k
   } else if (idx32) {
     if (k <= 8) {
       (ggp::count_launch(), knn_kernel<T, D, 8, int><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
-    } else if (k <= 16) {
-      constexpr size_t smem = 16 * 128 * KnnHeapSmem<T>::bytes_per_entry;
-      (ggp::count_launch(), knn_heap_kernel<T, D, 16, int><<<grid, 128, smem, s>>>(src, n, k, q, m, nq, q0, out));
     } else {
-      constexpr size_t smem = 32 * 128 * KnnHeapSmem<T>::bytes_per_entry;
-      auto kern = knn_heap_kernel<T, D, 32, int>;
-      allow_smem(kern, smem);
-      (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(src, n, k, q, m, nq, q0, out));
+      // the heap kernels refill lanes from a global query counter: one resident wave of blocks
+      const int max_blocks = (int)std::min<long long>((nq + 127) / 128, 1ll << 30);
+      cudaMemsetAsync(next_query, 0, sizeof(unsigned long long), s);
+      if (k <= 16) {
+        constexpr size_t smem = 16 * 128 * KnnHeapSmem<T>::bytes_per_entry;
+        auto kern = knn_heap_kernel<T, D, 16, int>;
+        allow_smem(kern, smem);
+        (ggp::count_launch(), kern<<<persistent_grid(kern, 128, smem, max_blocks), 128, smem, s>>>(src, n, k, q, m, nq, q0, out, next_query));
+      } else {
+        constexpr size_t smem = 32 * 128 * KnnHeapSmem<T>::bytes_per_entry;
+        auto kern = knn_heap_kernel<T, D, 32, int>;
+        allow_smem(kern, smem);
+        (ggp::count_launch(), kern<<<persistent_grid(kern, 128, smem, max_blocks), 128, smem, s>>>(src, n, k, q, m, nq, q0, out, next_query));
+      }
     }
   } else {
     if (k <= 8) (ggp::count_launch(), knn_kernel<T, D, 8, long long><<<grid, 128, 0, s>>>(src, n, k, q, m, nq, q0, out));
@@ -235,15 +246,16 @@ static int knn_device(const T* points, const int* split, long long n, int d, int
                       long long nq, long long q0, int* out, char* scratch, cudaStream_t s) {
   if (nq <= 0) return GGP_OK;
   NodeRec<T>* rec = nullptr;
-  knn_ws_bytes<T>(n, &rec, scratch);
+  unsigned long long* next_query = nullptr;
+  knn_ws_bytes<T>(n, &rec, scratch, &next_query);
   cudaError_t e;
   if (d <= 3) {
     (ggp::count_launch(), pack_nodes_kernel<T><<<g_grid(n), 256, 0, s>>>(points, split, n, d, rec));
-    if (d == 1) e = launch_knn_d<T, 1>(PointSource<T, 1>{rec, points, split, d}, n, k, q, m, nq, q0, out, s);
-    else if (d == 2) e = launch_knn_d<T, 2>(PointSource<T, 2>{rec, points, split, d}, n, k, q, m, nq, q0, out, s);
-    else e = launch_knn_d<T, 3>(PointSource<T, 3>{rec, points, split, d}, n, k, q, m, nq, q0, out, s);
+    if (d == 1) e = launch_knn_d<T, 1>(PointSource<T, 1>{rec, points, split, d}, n, k, q, m, nq, q0, out, next_query, s);
+    else if (d == 2) e = launch_knn_d<T, 2>(PointSource<T, 2>{rec, points, split, d}, n, k, q, m, nq, q0, out, next_query, s);
+    else e = launch_knn_d<T, 3>(PointSource<T, 3>{rec, points, split, d}, n, k, q, m, nq, q0, out, next_query, s);
   } else {
-    e = launch_knn_d<T, 0>(PointSource<T, 0>{nullptr, points, split, d}, n, k, q, m, nq, q0, out, s);
+    e = launch_knn_d<T, 0>(PointSource<T, 0>{nullptr, points, split, d}, n, k, q, m, nq, q0, out, next_query, s);
   }
   return g_status(e);
 }

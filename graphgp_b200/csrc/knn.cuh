@@ -209,35 +209,117 @@ template <typename T> struct KnnHeapSmem {
   static constexpr size_t bytes_per_entry = sizeof(T) + sizeof(int) + 1;
 };
 
+// Lanes are refilled: once no more than kKnnRefillAt lanes of a warp are still traversing (the stragglers),
+// every idle lane writes its finished result and takes a new query. The idle lanes take consecutive queries from
+// a global counter (one atomic per refill), so lanes refilled together start on neighbouring points and stay
+// coherent, and warps balance their load dynamically. A warp so runs close to the mean traversal length of its
+// lanes rather than waiting each time for its longest one (clustered points give queries of very different
+// lengths). The warp checks its lanes every kKnnStepsPerCheck traversal steps. Each query's traversal and
+// result are the same as with one query per thread.
+constexpr int kKnnRefillAt = 2;
+constexpr int kKnnStepsPerCheck = 16;
+static_assert(kKnnRefillAt < 32, "a refill needs an idle lane to fetch queries");
+
 template <typename T, int D, int KMAX, typename IDX>
 __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, long long n, int k,
                                                        const int* __restrict__ query_idx,
                                                        const int* __restrict__ max_idx, long long nq, long long q0,
-                                                       int* __restrict__ out) {
+                                                       int* __restrict__ out,
+                                                       unsigned long long* __restrict__ next_query) {
   constexpr int PD = D > 0 ? D : kKnnMaxD;
+  constexpr unsigned kFull = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char knn_smem[];
   const int bd = blockDim.x;
   T* hd = reinterpret_cast<T*>(knn_smem) + threadIdx.x;
   int* hi = reinterpret_cast<int*>(knn_smem + sizeof(T) * KMAX * bd) + threadIdx.x;
   unsigned char* hs = knn_smem + (sizeof(T) + sizeof(int)) * KMAX * bd + threadIdx.x;
   const T inf = (T)INFINITY;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += (long long)gridDim.x * blockDim.x) {
-    long long qi = query_idx ? (long long)query_idx[t] : q0 + t;
-    qi = qi < 0 ? 0 : (qi >= n ? n - 1 : qi);  // out-of-range query ids clamp like a JAX gather
-    long long mx = max_idx ? (long long)max_idx[t] : qi;
-    if (mx > n) mx = n;
-    T q[PD];
-    int qs;
-    src.load(qi, q, qs);
-    for (int e = 0; e < k; ++e) {
-      hd[e * bd] = inf;
-      hi[e * bd] = -1;
-      hs[e * bd] = (unsigned char)e;
+  const unsigned lanes_below = (1u << (threadIdx.x & 31)) - 1u;
+  bool more = true;      // warp-uniform: the counter has not yet passed nq
+  long long t = 0;       // this lane's query (output row)
+  bool live = false;     // traversal running
+  bool fin = false;      // traversal ended, result not yet written
+  T q[PD];
+  T maxv = inf;
+  IDX mxi = 0, cur = -1, prev = -1;
+  for (;;) {
+    const unsigned live_mask = __ballot_sync(kFull, live);
+    if (__popc(live_mask) <= kKnnRefillAt) {
+      if (fin) {
+        // order by (sqrt(d2), index) in the heap's own storage (keys replace the squared distances; entries
+        // past k hold (inf, INT_MAX) and sort last)
+        for (int j = 0; j < KMAX; ++j) {
+          if (j < k) {
+            T dd = hd[j * bd];
+            if (hi[j * bd] < 0) {
+              T p[PD];
+              int s;
+              src.load(n - 1, p, s);
+              dd = sqdist<T, D>(p, q, src.d);
+            }
+            hd[j * bd] = rn_sqrt(dd);
+          } else {
+            hd[j * bd] = inf;
+            hi[j * bd] = 0x7fffffff;
+          }
+        }
+#pragma unroll
+        for (int size = 2; size <= KMAX; size <<= 1) {
+#pragma unroll
+          for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+            for (int i = 0; i < KMAX; ++i) {
+              const int j = i ^ stride;
+              if (j > i) {
+                const T ki = hd[i * bd], kj = hd[j * bd];
+                const int ii = hi[i * bd], ij = hi[j * bd];
+                const bool j_less = (kj < ki) || (kj == ki && ij < ii);
+                const bool sw = ((i & size) == 0) ? j_less : !j_less;
+                if (sw) {
+                  hd[i * bd] = kj; hd[j * bd] = ki;
+                  hi[i * bd] = ij; hi[j * bd] = ii;
+                }
+              }
+            }
+          }
+        }
+        int* o = out + t * k;
+        for (int j = 0; j < k; ++j) o[j] = hi[j * bd];
+        fin = false;
+      }
+      const unsigned idle = ~live_mask;
+      long long base = nq;  // no new query once the counter has passed nq
+      if (more) {
+        const int leader = __ffs(idle) - 1;  // idle is never empty here: at most kKnnRefillAt < 32 lanes live
+        if ((int)(threadIdx.x & 31) == leader) base = (long long)atomicAdd(next_query, (unsigned long long)__popc(idle));
+        base = __shfl_sync(kFull, base, leader);
+        more = base + __popc(idle) < nq;
+      }
+      if (!live) {
+        t = base + __popc(idle & lanes_below);
+        if (t < nq) {
+          long long qi = query_idx ? (long long)query_idx[t] : q0 + t;
+          qi = qi < 0 ? 0 : (qi >= n ? n - 1 : qi);  // out-of-range query ids clamp like a JAX gather
+          long long mx = max_idx ? (long long)max_idx[t] : qi;
+          if (mx > n) mx = n;
+          int qs;
+          src.load(qi, q, qs);
+          for (int e = 0; e < k; ++e) {
+            hd[e * bd] = inf;
+            hi[e * bd] = -1;
+            hs[e * bd] = (unsigned char)e;
+          }
+          maxv = inf;
+          mxi = (IDX)mx;
+          cur = mx > 0 ? 0 : -1;
+          prev = -1;
+          live = cur != -1;
+          fin = !live;  // a query with no preceding points still writes its (unfilled) result
+        }
+      }
+      if (__ballot_sync(kFull, live || fin) == 0) break;
     }
-    T maxv = inf;
-    const IDX mxi = (IDX)mx;
-    IDX cur = mx > 0 ? 0 : -1, prev = -1;
-    while (cur != -1) {
+    for (int r = 0; r < kKnnStepsPerCheck && live; ++r) {
       const IDX par = tree_parent(cur);
       T p[PD];
       int s;
@@ -284,46 +366,11 @@ __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, lo
       else next = (prev == par) ? nearc : par;
       prev = cur;
       cur = next;
-    }
-    // order by (sqrt(d2), index) in the heap's own storage (keys replace the squared distances; entries past k
-    // hold (inf, INT_MAX) and sort last)
-    for (int j = 0; j < KMAX; ++j) {
-      if (j < k) {
-        T dd = hd[j * bd];
-        if (hi[j * bd] < 0) {
-          T p[PD];
-          int s;
-          src.load(n - 1, p, s);
-          dd = sqdist<T, D>(p, q, src.d);
-        }
-        hd[j * bd] = rn_sqrt(dd);
-      } else {
-        hd[j * bd] = inf;
-        hi[j * bd] = 0x7fffffff;
+      if (cur == -1) {
+        live = false;
+        fin = true;
       }
     }
-#pragma unroll
-    for (int size = 2; size <= KMAX; size <<= 1) {
-#pragma unroll
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-#pragma unroll
-        for (int i = 0; i < KMAX; ++i) {
-          const int j = i ^ stride;
-          if (j > i) {
-            const T ki = hd[i * bd], kj = hd[j * bd];
-            const int ii = hi[i * bd], ij = hi[j * bd];
-            const bool j_less = (kj < ki) || (kj == ki && ij < ii);
-            const bool sw = ((i & size) == 0) ? j_less : !j_less;
-            if (sw) {
-              hd[i * bd] = kj; hd[j * bd] = ki;
-              hi[i * bd] = ij; hi[j * bd] = ii;
-            }
-          }
-        }
-      }
-    }
-    int* o = out + t * k;
-    for (int j = 0; j < k; ++j) o[j] = hi[j * bd];
   }
 }
 
