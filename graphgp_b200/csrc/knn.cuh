@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long lo
     T maxv = inf;
     int maxj = 0;
     const IDX mxi = (IDX)mx;
-    IDX cur = mx > 0 ? 0 : -1, prev = -1;
+    IDX cur = 0, prev = -1;  // the root is visited whatever the limit (tree.py _traverse_tree starts there)
     while (cur != -1) {
       const IDX par = tree_parent(cur);
       T p[PD];
@@ -311,10 +311,9 @@ __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, lo
           }
           maxv = inf;
           mxi = (IDX)mx;
-          cur = mx > 0 ? 0 : -1;
+          cur = 0;  // the root is visited whatever the limit (tree.py _traverse_tree starts there)
           prev = -1;
-          live = cur != -1;
-          fin = !live;  // a query with no preceding points still writes its (unfilled) result
+          live = true;
         }
       }
       if (__ballot_sync(kFull, live || fin) == 0) break;
@@ -402,7 +401,7 @@ __global__ void __launch_bounds__(128) knn_kernel_wide(PointSource<T, D> src, lo
     for (int j = 0; j < k; ++j) { nb[j] = -1; dv[j] = inf; }
     T maxv = inf;
     int maxj = 0;
-    long long cur = mx > 0 ? 0 : -1, prev = -1;
+    long long cur = 0, prev = -1;  // the root is visited whatever the limit
     while (cur != -1) {
       const long long par = tree_parent(cur);
       T p[PD];

@@ -108,17 +108,24 @@ def test_query_preceding_brute_force(cuda_device):
     assert np.array_equal(nb, true)
 
 
-def test_query_neighbors_arbitrary(cuda_device):
+@pytest.mark.parametrize("k,small_max", [(12, False), (32, True), (16, True)])
+def test_query_neighbors_arbitrary(cuda_device, k, small_max):
+    """Arbitrary query ids and per-query search limits. ``small_max`` adds limits of 0 (only the root is visited,
+    as in the reference's traversal) and below k (unfilled slots, ordered against the last point like the
+    reference)."""
     from graphgp_b200 import graphgp_cuda as gc
 
     pts = np.random.default_rng(3).standard_normal((5000, 3)).astype(np.float32)
     rp, rs, _ = ot.build_tree(pts)
-    rng = np.random.default_rng(4)
+    rng = np.random.default_rng(4 + k)
     q = rng.integers(0, 5000, 700)
-    m = np.maximum(rng.integers(0, 5000, 700), 12)
+    m = np.maximum(rng.integers(0, 5000, 700), k)
+    if small_max:
+        m[:60] = rng.integers(0, 2 * k, 60)
+        m[:5] = 0
     out = _np(gc.query_neighbors(_t(rp, cuda_device), _t(rs, cuda_device), _t(q.astype(np.int32), cuda_device),
-                                 _t(m.astype(np.int32), cuda_device), k=12))
-    ref = ot.query_neighbors(rp, rs, q, m, k=12)
+                                 _t(m.astype(np.int32), cuda_device), k=k))
+    ref = ot.query_neighbors(rp, rs, q, m, k=k)
     assert np.array_equal(out, ref)
 
 
