@@ -27,39 +27,48 @@ __global__ void __launch_bounds__(256) depths_kernel(const int* __restrict__ nbr
     bool bad = false;
     if (valid) {
       // neighbours in groups of 32: the ids, then their depths, are loaded back to back, so a row costs two
-      // round trips to L2 per group instead of two per neighbour on the chain of dependent rows
+      // round trips to L2 per group instead of two per neighbour on the chain of dependent rows. Depths still
+      // pending are polled together from one loop, so the waiting lanes of a warp share one wait site.
       for (int m0 = 0; m0 < k; m0 += 32) {
-        int ids[32], vs[32];
+        int ids[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) ids[j] = m0 + j < k ? nr[m0 + j] : -1;
+        unsigned int pend = 0;
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
           const bool in = ids[j] >= 0 && (long long)ids[j] < row;
           if (m0 + j < k && !in) bad = true;
-          if (!in) ids[j] = -1;
-          vs[j] = in ? ld_relaxed(depth + ids[j]) : -1;
+          if (in) {
+            const int v = ld_relaxed(depth + ids[j]);
+            if (v < 0) pend |= 1u << j;
+            else ext = v > ext ? v : ext;
+          }
         }
+        // a neighbour inside this chunk is a lower lane of this warp, which stores its depth as soon as it is
+        // known; the divergent lanes of a warp progress independently, and every wait is bounded
+        if (pend) {
+          const uint64_t t0 = global_timer_ns();
+          unsigned int backoff = 32;
+          while (pend) {
+            __nanosleep(backoff);
+            if (backoff < 256) backoff <<= 1;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          if (ids[j] < 0) continue;
-          int v = vs[j];
-          // a neighbour inside this chunk is a lower lane of this warp, which stores its depth as soon as it
-          // is known; the divergent lanes of a warp progress independently, and every wait is bounded
-          if (v < 0) {
-            const uint64_t t0 = global_timer_ns();
-            unsigned int backoff = 32;
-            while (v < 0) {
-              __nanosleep(backoff);
-              if (backoff < 256) backoff <<= 1;
-              v = ld_relaxed(depth + ids[j]);
-              if (v < 0 && global_timer_ns() - t0 > timeout_ns) {
-                atomicAdd(&st->timeouts, 1u);
-                report_error(st, GGP_ERR_TIMEOUT);
-                v = 0;
+            for (int j = 0; j < 32; ++j) {
+              if (pend & (1u << j)) {
+                const int v = ld_relaxed(depth + ids[j]);
+                if (v >= 0) {
+                  ext = v > ext ? v : ext;
+                  pend &= ~(1u << j);
+                }
               }
             }
+            if (pend && global_timer_ns() - t0 > timeout_ns) {
+              atomicAdd(&st->timeouts, 1u);
+              report_error(st, GGP_ERR_TIMEOUT);
+              pend = 0;  // the missing depths count as 0
+              ext = ext > 0 ? ext : 0;
+            }
           }
-          ext = v > ext ? v : ext;
         }
       }
     }
