@@ -183,18 +183,44 @@ __device__ __forceinline__ T quad_mean(const RefineParams<T>& p, bool gen, bool 
     if (i < K && ids[t] >= 0) val[t] = gen ? ld_relaxed(p.values + ids[t]) : __ldg(p.values + ids[t]);
   }
   if (gen) {
+    unsigned int pend = 0;
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       const int i = t * kQuad + g;
-      if (i < K && ids[t] >= 0 && is_pending(val[t])) {
-        T v;
-        if (may_wait) {
-          ok &= wait_ready(p.values + ids[t], v, p.timeout_ns);
-        } else {
-          ok = false;
-          v = T(0);
+      if (i < K && ids[t] >= 0 && is_pending(val[t])) pend |= 1u << t;
+    }
+    if (pend && !may_wait) {
+      ok = false;
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+        if (pend & (1u << t)) val[t] = T(0);
+      pend = 0;
+    }
+    // the values still pending are polled together from one loop (bounded), so the waiting lanes of a warp
+    // share one wait site; a value that never arrives becomes NaN and the point reports the timeout
+    if (pend) {
+      const uint64_t t0 = global_timer_ns();
+      unsigned int backoff = 32;
+      while (pend) {
+        __nanosleep(backoff);
+        if (backoff < 512) backoff <<= 1;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+          if (pend & (1u << t)) {
+            const T v = ld_relaxed(p.values + ids[t]);
+            if (!is_pending(v)) {
+              val[t] = v;
+              pend &= ~(1u << t);
+            }
+          }
         }
-        val[t] = v;
+        if (pend && global_timer_ns() - t0 > p.timeout_ns) {
+          ok = false;
+#pragma unroll
+          for (int t = 0; t < NT; ++t)
+            if (pend & (1u << t)) val[t] = canonical(val[t] + (T)NAN);
+          pend = 0;
+        }
       }
     }
   }
