@@ -334,9 +334,9 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "kernel": "refine_quad2_kernel<float,16,3> (generate mode)",
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at N = 4,194,304 "
-                                       "(189.4 B per refined point), scaled to this launch's refined points",
+                                       "(190.3 B per refined point), scaled to this launch's refined points",
                      "note": "bound by instruction issue and latency, not HBM (44% issue-active, 20 of 64 warps "
-                             "resident in the ncu capture; 43% of the instruction-issue bound)",
+                             "resident in the ncu capture; 44% of the instruction-issue bound)",
                      "kernel_ms": kern_ms, "algorithmic_bytes_per_point": BYTES_PER_POINT,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
         "gpu_launches": launches,
