@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256) depths_kernel(const int* __restrict__ nbr
         if (pend) {
           const uint64_t t0 = global_timer_ns();
           unsigned int backoff = 32;
-          while (pend) {
+          for (unsigned int it = 0; pend; ++it) {
             __nanosleep(backoff);
             if (backoff < 256) backoff <<= 1;
 #pragma unroll
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) depths_kernel(const int* __restrict__ nbr
                 }
               }
             }
-            if (pend && global_timer_ns() - t0 > timeout_ns) {
+            if (pend && (global_timer_ns() - t0 > timeout_ns || it >= (1u << 30))) {
               atomicAdd(&st->timeouts, 1u);
               report_error(st, GGP_ERR_TIMEOUT);
               pend = 0;  // the missing depths count as 0

@@ -187,8 +187,8 @@ RefineParams<T> make_params(const Workspace& ws, const T* points, long long n, i
   p.chunk_prefix = ws.chunk_prefix;
   p.tb = ws.table;
   p.status = ws.status;
-  p.tau = tau;
-  p.timeout_ns = timeout_ns ? timeout_ns : 10000000000ull;
+  p.tau = tau < 0 ? GGP_DEFAULT_TAU : tau;  // a negative tau selects the default (inverse calls resolve it first)
+  p.timeout_ns = timeout_ns ? (timeout_ns < GGP_MAX_TIMEOUT_NS ? timeout_ns : GGP_MAX_TIMEOUT_NS) : 10000000000ull;
   p.logdet_partials = ws.partials;
   return p;
 }
@@ -293,6 +293,7 @@ int refine_inv_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t
   int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !values || !out_init || (n > n0 && !out_xi)) return GGP_ERR_INVALID;
+  if (tau < 0) tau = GGP_DEFAULT_TAU_INVERSE;
   Workspace ws;
   rc = carve_workspace(GGP_OP_REFINE_INV, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
   if (rc) return rc;
@@ -371,6 +372,7 @@ int generate_inv_impl(const T* points, const int32_t* perm, int64_t n, int d, in
   int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !values || !out_xi) return GGP_ERR_INVALID;
+  if (tau < 0) tau = GGP_DEFAULT_TAU_INVERSE;
   Workspace ws;
   rc = carve_workspace(GGP_OP_GENERATE_INV, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
   if (rc) return rc;
@@ -670,36 +672,81 @@ int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n
 // scratch allocator, or a latency-critical loop that must never enter an allocator. For them this entry
 // point runs the same refine_logdet computation with its scratch taken from a fixed array in device memory
 // that the library owns: kNoAllocScratchBytes (1 MiB) on every GPU that loads the library, held until the
-// process exits. That bounds the table to 4097 entries and the offsets array to 100,000 entries; larger
-// inputs are rejected with GGP_ERR_UNSUPPORTED before anything runs.
+// process exits. Inputs are limited to kNoAllocMaxBins (4097) table entries and kNoAllocMaxOffsets (100,000)
+// offsets, each checked on its own; together they need about 650 KiB of the array. Larger inputs are rejected
+// with GGP_ERR_UNSUPPORTED before anything runs.
 //
 // The array's name is only meaningful to device code; host code needs its device address, which the first
-// call on each device looks up (cudaGetSymbolAddress, with that device current) and caches. Make that first
-// call on each device before any stream capture. Every call on a device shares the one array and leaves its
-// contents behind; each call clears what has to start at zero (the status block and the partial sums)
-// itself, but calls whose work overlaps on the GPU (different streams, or host threads) race on the array
-// and must be serialised by the caller.
+// call on each device looks up (cudaGetSymbolAddress, with that device current) and caches together with the
+// identity of the device's current context. A call that finds another context (the device was reset and its
+// context re-created, which reloads the module) looks the address up again. Make the first call on each device
+// before any stream capture. Every call on a device shares the one array and leaves its contents behind; each
+// call clears what has to start at zero (the status block and the partial sums) itself, but calls whose work
+// overlaps on the GPU (different streams, or host threads) race on the array and must be serialised by the
+// caller. The status block is in the array, so device-side failures reach the caller only as a NaN result.
 // ------------------------------------------------------------------------------------------------
 #include <mutex>
 
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;
+constexpr int kNoAllocMaxBins = 4097;
+constexpr int kNoAllocMaxOffsets = 100000;
 constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+// The largest inputs the limits allow must fit the array whatever the other sizes are.
+static_assert(256 + (kNoAllocMaxBins - 1) * 48 + 2 * 2 * kHintMax + 4 * 256 + 4 * (kNoAllocMaxOffsets + 2) +
+                      8 * kMaxPartials + 4 * 256 <=
+                  kNoAllocScratchBytes,
+              "no-allocation limits exceed the static scratch array");
 
-// Device address of g_noalloc_scratch on the current device (looked up once per device).
+// Driver entry points for the current context's unique id (cuCtxGetCurrent, cuCtxGetId), looked up through the
+// runtime so that the library needs no link against the driver library.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+
+struct NoAllocSlot {
+  void* ptr = nullptr;
+  unsigned long long ctx_id = 0;
+};
+
+std::mutex g_noalloc_mutex;
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
+
+// Id of the current context, or 0 when it cannot be read (the cache then holds one address per device).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device and context.
 int noalloc_scratch(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_status(e);
   if (dev < 0 || dev >= kNoAllocMaxDevices) return GGP_ERR_UNSUPPORTED;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
+  NoAllocSlot& slot = g_noalloc_slot[dev];
+  const unsigned long long id = current_context_id();
+  if (!slot.ptr || (id != 0 && id != slot.ctx_id)) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -707,9 +754,11 @@ int noalloc_scratch(void** out) {
               cudaGetErrorString(e));
       return GGP_ERR_CUDA;
     }
-    g_noalloc_ptr[dev] = p;
+    slot.ptr = p;
+    // the lookup made the device's primary context current if none was: read the id it has now
+    slot.ctx_id = id != 0 ? id : current_context_id();
   }
-  *out = g_noalloc_ptr[dev];
+  *out = slot.ptr;
   return GGP_OK;
 }
 
@@ -719,18 +768,20 @@ extern "C" int ggp_refine_logdet_f32_noalloc(const float* points, int64_t n, int
                                              const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                                              const float* cov_bins, const float* cov_vals, int n_bins,
                                              double* out_logdet, double tau, ggp_stream_t stream) {
-  Workspace need;
-  carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, n_bins < 2 ? 2 : n_bins, n_offsets < 1 ? 1 : n_offsets, 4,
-                  nullptr, 0, &need);
-  if (need.total > kNoAllocScratchBytes) {
+  int rc = check_refine_args(points, n, d, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins);
+  if (rc) return rc;
+  if (n_bins > kNoAllocMaxBins || n_offsets > kNoAllocMaxOffsets) {
     fprintf(stderr,
-            "graphgp_b200: ggp_refine_logdet_f32_noalloc needs %zu bytes of scratch, more than its fixed %zu "
-            "(at most 4097 table entries and 100000 offsets); use ggp_refine_logdet_f32 with a workspace\n",
-            need.total, kNoAllocScratchBytes);
+            "graphgp_b200: ggp_refine_logdet_f32_noalloc takes at most %d table entries and %d offsets (got %d and "
+            "%d); use ggp_refine_logdet_f32 with a workspace\n",
+            kNoAllocMaxBins, kNoAllocMaxOffsets, n_bins, n_offsets);
     return GGP_ERR_UNSUPPORTED;
   }
+  Workspace need;
+  carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, n_bins, n_offsets, 4, nullptr, 0, &need);
+  if (need.total > kNoAllocScratchBytes) return GGP_ERR_UNSUPPORTED;  // unreachable under the limits above
   void* scratch = nullptr;
-  int rc = noalloc_scratch(&scratch);
+  rc = noalloc_scratch(&scratch);
   if (rc) return rc;
   return refine_logdet_impl<float>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
                                    out_logdet, tau, scratch, kNoAllocScratchBytes, GGP_STREAM(stream));

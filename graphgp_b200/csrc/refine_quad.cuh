@@ -201,7 +201,8 @@ __device__ __forceinline__ T quad_mean(const RefineParams<T>& p, bool gen, bool 
     if (pend) {
       const uint64_t t0 = global_timer_ns();
       unsigned int backoff = 32;
-      while (pend) {
+      // ends on the time limit (clamped on the host) or, whatever the timer does, after 2^30 polls
+      for (unsigned int it = 0; pend; ++it) {
         __nanosleep(backoff);
         if (backoff < 512) backoff <<= 1;
 #pragma unroll
@@ -214,7 +215,7 @@ __device__ __forceinline__ T quad_mean(const RefineParams<T>& p, bool gen, bool 
             }
           }
         }
-        if (pend && global_timer_ns() - t0 > p.timeout_ns) {
+        if (pend && (global_timer_ns() - t0 > p.timeout_ns || it >= (1u << 30))) {
           ok = false;
 #pragma unroll
           for (int t = 0; t < NT; ++t)

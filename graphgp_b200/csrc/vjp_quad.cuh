@@ -198,10 +198,10 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
       if (lane == 0 && !waited_out) {
         const uint64_t t_start = global_timer_ns();
         unsigned int backoff = 32;
-        while ((unsigned int)ld_acquire_u32(&p.status->done) < need) {
+        for (unsigned int it = 0; (unsigned int)ld_acquire_u32(&p.status->done) < need; ++it) {
           __nanosleep(backoff);
           if (backoff < 512) backoff <<= 1;
-          if (global_timer_ns() - t_start > p.timeout_ns) {
+          if (global_timer_ns() - t_start > p.timeout_ns || it >= (1u << 30)) {
             atomicAdd(&p.status->timeouts, 1u);
             report_error(p.status, GGP_ERR_TIMEOUT);
             waited_out = true;

@@ -143,10 +143,19 @@ int ggp_build_graph_f64(const double* points, int64_t n, int d, int64_t n0, int 
 /* ---------------------------------------------------------------------------------------------- */
 /* Refinement (reference graphgp/refine.py)                                                        */
 /* `offsets` is the reference's offsets tuple as a device array (refine.py:120): n_offsets entries,   */
-/* offsets[0] = n0, offsets[n_offsets-1] = n; n0 = n - rows(neighbors) (refine.py:111). `tau`: a point whose smallest pivot ratio              */
-/* (Schur complement / variance) falls below tau is re-conditioned in FP64 (f32 functions only;       */
-/* 0 disables). `timeout_ns` bounds every wait of a point on a neighbour value (0 = default 10 s).   */
+/* offsets[0] = n0, offsets[n_offsets-1] = n; n0 = n - rows(neighbors) (refine.py:111).              */
+/* `tau` (f32 functions only): a point whose smallest pivot ratio (Schur complement / prior variance) */
+/* falls below tau is re-conditioned in FP64; 0 disables it, a negative value selects the default of  */
+/* the operation: GGP_DEFAULT_TAU for generate and log-determinant, GGP_DEFAULT_TAU_INVERSE for the   */
+/* inverse. The inverse needs the larger threshold because xi = (v - mean) / std divides the FP32     */
+/* rounding of the mean by std: with smooth kernels most pivot ratios sit near the jitter (1e-4), and */
+/* a pure FP32 inverse then misses 1e-4 relative error (FP32 NumPy gets 4e-4 on such graphs).         */
+/* `timeout_ns` bounds every wait of a point on a neighbour value (0 = default 10 s; values above     */
+/* GGP_MAX_TIMEOUT_NS are clamped to it).                                                           */
 /* ---------------------------------------------------------------------------------------------- */
+#define GGP_DEFAULT_TAU 1e-5
+#define GGP_DEFAULT_TAU_INVERSE 3e-3
+#define GGP_MAX_TIMEOUT_NS 300000000000ull /* 300 s */
 
 /* graphgp_cuda.refine(points, neighbors, offsets, cov_bins, cov_vals, initial_values, xi) --
  * graphgp/refine.py:119-121 (semantics 123-159). out_values (n,) in graph order. */
@@ -185,10 +194,14 @@ int ggp_refine_logdet_f64(const double* points, int64_t n, int d, int64_t n0, co
  * Frameworks that reserve nearly all of the GPU for their own memory pool, foreign-function handlers that
  * are given no scratch allocator, and loops that must not enter an allocator can call this instead: it takes
  * no workspace and uses a fixed 1 MiB array of device memory owned by the library (held on every GPU that
- * loads it until exit), so inputs are limited to 4097 table entries and 100000 offsets (larger ones return
- * GGP_ERR_UNSUPPORTED). The first call on each device looks up the array's address; make it before any
- * stream capture. All calls on a device share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. *out_logdet is a device double. */
+ * loads it until exit), so inputs are limited to n_bins <= 4097 table entries and n_offsets <= 100000
+ * offsets, each checked on its own (larger ones return GGP_ERR_UNSUPPORTED before anything runs). The
+ * first call on each device (and the first after that device's context was reset and re-created) looks up
+ * the array's address; make it before any stream capture. All calls on a device share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller. *out_logdet is a device double. The
+ * status block lives in the library's array, not in a caller buffer, so there is no ggp_read_status for
+ * these calls: a failure only the device sees (a malformed graph, a non-positive pivot) shows up as a NaN
+ * log-determinant. */
 int ggp_refine_logdet_f32_noalloc(const float* points, int64_t n, int d, int64_t n0, const int32_t* neighbors,
                                   int k, const int32_t* offsets, int n_offsets, const float* cov_bins,
                                   const float* cov_vals, int n_bins, double* out_logdet, double tau,

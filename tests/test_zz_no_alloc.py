@@ -83,17 +83,55 @@ def test_noalloc_logdet_matches_workspace_version_twice(cuda_device, n, d, n0, k
     assert abs(second - oracle) <= TOL32 * abs(oracle)
 
 
-def test_noalloc_refuses_inputs_beyond_its_scratch(cuda_device):
+def _call_noalloc(lib, dev, P, n, d, n0, NB, k, OF, nofs, B, V, nb):
+    import torch
+
+    out = torch.full((), float("nan"), dtype=torch.float64, device=dev)
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = lib.ggp_refine_logdet_f32_noalloc(C.c_void_p(P.data_ptr()), n, d, n0, C.c_void_p(NB.data_ptr()), k,
+                                           C.c_void_p(OF.data_ptr()), nofs, C.c_void_p(B.data_ptr()),
+                                           C.c_void_p(V.data_ptr()), nb, C.c_void_p(out.data_ptr()), 1e-5, s)
+    return rc, out
+
+
+def test_noalloc_limits_at_the_boundary(cuda_device):
+    """The two stated limits, each on its own: 4097 table entries together with 100,000 offsets is accepted and
+    gives the same log-determinant as the workspace version; 100,001 offsets or 4098 table entries is refused
+    before anything runs. The offsets are the graph's own, padded with empty batches at the end (allowed: a
+    batch may be empty, and the log-determinant waits on nothing)."""
+    import torch
+
     from graphgp_b200 import _lib
 
     lib = _lib.load()
-    args, _, _ = _inputs(cuda_device, 3000, 3, 256, 16)
-    (P, n, d, n0, NB, k, OF, nofs, B, V, nb) = args
-    import torch
+    pts, g = oracle_graph(3000, 3, 256, 16)
+    P = _t(g.points, cuda_device)
+    NB = _t(g.neighbors.astype(np.int32), cuda_device)
+    f32 = torch.float32
 
-    out = torch.empty((), dtype=torch.float64, device=cuda_device)
-    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    rc = lib.ggp_refine_logdet_f32_noalloc(C.c_void_p(P.data_ptr()), n, d, n0, C.c_void_p(NB.data_ptr()), k,
-                                           C.c_void_p(OF.data_ptr()), 400000, C.c_void_p(B.data_ptr()),
-                                           C.c_void_p(V.data_ptr()), nb, C.c_void_p(out.data_ptr()), 1e-5, s)
+    def table(nb):
+        bins, vals = matern32_table(cutoff=0.5, n_bins=nb)
+        return _t(bins, cuda_device, f32), _t(vals, cuda_device, f32)
+
+    def padded(count):
+        offs = np.asarray(g.offsets, np.int32)
+        return _t(np.concatenate([offs, np.full(count - len(offs), offs[-1], np.int32)]), cuda_device)
+
+    B, V = table(4097)
+    OF = padded(100000)
+    args = (P, 3000, 3, 256, NB, 16, _t(np.asarray(g.offsets, np.int32), cuda_device), len(g.offsets), B, V, 4097)
+    ref = _logdet_with_workspace(lib, args, cuda_device)
+    rc, out = _call_noalloc(lib, cuda_device, P, 3000, 3, 256, NB, 16, OF, 100000, B, V, 4097)
+    assert rc == 0
+    assert abs(float(out) - ref) <= TOL32 * abs(ref)
+
+    OF1 = padded(100001)
+    rc, out = _call_noalloc(lib, cuda_device, P, 3000, 3, 256, NB, 16, OF1, 100001, B, V, 4097)
     assert rc == _lib.GGP_ERR_UNSUPPORTED
+    B2, V2 = table(4098)
+    rc, out = _call_noalloc(lib, cuda_device, P, 3000, 3, 256, NB, 16, OF, 100000, B2, V2, 4098)
+    assert rc == _lib.GGP_ERR_UNSUPPORTED
+    rc, out = _call_noalloc(lib, cuda_device, P, 3000, 3, 256, NB, 16, OF, 400000, B, V, 4097)
+    assert rc == _lib.GGP_ERR_UNSUPPORTED
+    torch.cuda.synchronize()
+    assert torch.isnan(out).item()  # refused calls write nothing
