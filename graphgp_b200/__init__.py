@@ -3,7 +3,7 @@
 The names below are the reference's public API (graphgp/__init__.py), on CUDA torch tensors; the C ABI is
 declared in include/graphgp_b200.h and bound by ``graphgp_b200.graphgp_cuda``.
 """
-from . import extras
+from . import autograd, extras
 from .api import (
     Graph,
     build_graph,
@@ -12,6 +12,7 @@ from .api import (
     compute_cov_matrix,
     compute_depths,
     generate,
+    generate_and_logdet,
     generate_dense,
     generate_dense_inv,
     generate_dense_logdet,
@@ -30,7 +31,7 @@ from .api import (
 
 __all__ = [
     "build_tree", "query_preceding_neighbors", "query_neighbors", "Graph", "check_graph", "build_graph",
-    "compute_depths", "order_by_depth", "generate", "generate_inv", "generate_logdet", "generate_dense",
+    "compute_depths", "order_by_depth", "generate", "generate_and_logdet", "generate_inv", "generate_logdet", "generate_dense",
     "generate_dense_inv", "generate_dense_logdet", "refine", "refine_inv", "refine_logdet", "compute_cov_matrix",
-    "generate_vjp", "save_graph", "load_graph", "extras",
+    "generate_vjp", "save_graph", "load_graph", "extras", "autograd",
 ]

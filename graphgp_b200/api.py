@@ -7,8 +7,9 @@ Same names, argument meaning, results and errors as the reference's ``cuda=True`
 ``compute_cov_matrix`` (reference graph.py:20-137, tree.py:19-76, refine.py:21-305). A covariance is the pair
 ``(cov_bins, cov_vals)``. There is no CPU path: ``cuda=False`` raises.
 
-Beyond the reference: ``generate_vjp`` (the adjoint), and ``save_graph`` / ``load_graph`` to keep a built
-graph across processes as an ``.npz`` file.
+Beyond the reference: ``generate_vjp`` (the adjoint, which also backs autograd through ``generate``,
+``generate_logdet`` and ``generate_and_logdet``), and ``save_graph`` / ``load_graph`` to keep a built graph across
+processes as an ``.npz`` file.
 """
 from __future__ import annotations
 
@@ -18,6 +19,7 @@ from typing import Optional, Tuple
 import numpy as np
 import torch
 
+from . import autograd as _ag
 from . import graphgp_cuda as _gc
 
 
@@ -85,10 +87,19 @@ def order_by_depth(points, indices, neighbors, depths, *, cuda: bool = True):
     return _gc.order_by_depth(points, indices, neighbors, depths)
 
 
+def _wants_grad(*ts):
+    return torch.is_grad_enabled() and any(isinstance(t, torch.Tensor) and t.requires_grad for t in ts)
+
+
 def generate(graph: Graph, covariance, xi, *, cuda: bool = True, fast_jit: bool = True):
     """Values (N,) in the original point order (reference refine.py:21-56). ``fast_jit`` has one meaning here:
-    both of the reference's forms compute the same values."""
+    both of the reference's forms compute the same values. Differentiable: when ``xi`` or the table values
+    require grad, the call is recorded for autograd and its backward runs the adjoint kernels
+    (``graphgp_b200.autograd.GenerateFn``)."""
     _need_cuda(cuda)
+    if _wants_grad(xi, covariance[1]):
+        return _ag.generate(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0],
+                            covariance[1], xi)
     return _gc.generate(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0], covariance[1],
                         xi)
 
@@ -101,9 +112,25 @@ def generate_inv(graph: Graph, covariance, values, *, cuda: bool = True):
 
 
 def generate_logdet(graph: Graph, covariance, *, cuda: bool = True):
-    """Log-determinant of the generate map, FP64 (reference refine.py:234-240)."""
+    """Log-determinant of the generate map, FP64 (reference refine.py:234-240). Differentiable in the table
+    values (``graphgp_b200.autograd.GenerateLogdetFn``)."""
     _need_cuda(cuda)
+    if _wants_grad(covariance[1]):
+        return _ag.generate_logdet(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0],
+                                   covariance[1])
     return _gc.generate_logdet(graph.points, graph.neighbors, graph.offsets, covariance[0], covariance[1])
+
+
+def generate_and_logdet(graph: Graph, covariance, xi, *, cuda: bool = True):
+    """``(generate(graph, covariance, xi), generate_logdet(graph, covariance))`` in one call; under autograd the
+    backward pass runs a single adjoint sweep for both outputs (a likelihood 0.5|v - y|^2 + logdet)."""
+    _need_cuda(cuda)
+    if _wants_grad(xi, covariance[1]):
+        return _ag.generate_and_logdet(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0],
+                                       covariance[1], xi)
+    return (_gc.generate(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0], covariance[1],
+                         xi),
+            _gc.generate_logdet(graph.points, graph.neighbors, graph.offsets, covariance[0], covariance[1]))
 
 
 def generate_vjp(graph: Graph, covariance, xi, g_values, g_logdet: float = 0.0, *, values=None):

@@ -34,7 +34,10 @@ struct DeviceStatus {
   unsigned int ticket;         // work counter for persistent kernels
   unsigned int ticket2;        // second work counter (reverse sweep of the adjoint)
   unsigned int done;           // chunks finished by the reverse sweep
-  unsigned int pad[57];        // keeps the struct at 256 bytes
+  unsigned int listed;         // rows the FP32 inverse / logdet left to the FP64 second pass
+  unsigned int bar_count;      // grid barrier of the dense-root kernel: blocks arrived
+  unsigned int bar_gen;        // grid barrier of the dense-root kernel: generation
+  unsigned int pad[54];        // keeps the struct at 256 bytes
 };
 static_assert(sizeof(DeviceStatus) == 256, "status block must be 256 bytes");
 

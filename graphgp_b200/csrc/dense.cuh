@@ -1,9 +1,17 @@
 // Dense root in FP64 on the GPU: the n0 x n0 covariance of the first n0 points, its Cholesky factor, and
 // L @ xi / L^-1 v / sum log L_ii (reference graphgp/refine.py:59-76, 186-195, 243-248).
 //
-// Blocked right-looking Cholesky on a row-major n0 x n0 matrix (lower triangle used) with 64 x 64 tiles:
-// per panel p, one block factors the diagonal tile in shared memory, one block per tile row solves the
-// panel below it (X L_pp^T = A_ip), and one block per lower trailing tile applies A_ij -= A_ip A_jp^T.
+// Blocked right-looking Cholesky on a row-major n0 x n0 matrix (lower triangle used; the upper triangle is never
+// written or read) with 64 x 64 tiles, all in one cooperative kernel: the whole dense root is one launch with no
+// host round trip between panels. Per panel p:
+//   1. every block with a tile row below the panel (and block 0) factors the diagonal tile A_pp in shared memory
+//      (the same small factorisation, repeated, instead of a broadcast step); block t solves tile row p + 1 + t,
+//      L_ip = A_ip L_pp^-T, and writes it;
+//   2. grid barrier; block 0 writes L_pp; every block takes trailing tiles (i, j), p < j <= i, A_ij -= L_ip L_jp^T;
+//   3. grid barrier.
+// Two barriers per panel replace three kernel launches per panel. The barrier is a sense-reversing counter in the
+// status block whose waits are bounded (a wait that runs out records GGP_ERR_TIMEOUT and ends the block); the
+// launch is cooperative, so every block is resident and the barrier always completes.
 #pragma once
 
 #include "table.cuh"
@@ -12,89 +20,121 @@ namespace ggp {
 
 constexpr int kDenseTile = 64;
 
-template <typename TP>
-__global__ void dense_cov_kernel(const TP* __restrict__ points, long long n0, int d, const int* __restrict__ perm,
-                                 TableBuffers tb, double* __restrict__ A) {
-  const TableView<double> tab = global_table_view<double>(tb);
-  const double c0 = tb.desc->c0;
-  const long long total = n0 * n0;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    const long long i = e / n0, j = e - i * n0;
-    double v;
-    if (i == j) {
-      v = c0;
-    } else {
-      const long long a = i, b = j;
-      double s2 = 0.0;
-      for (int c = 0; c < d; ++c) {
-        const double df = (double)points[a * d + c] - (double)points[b * d + c];
-        s2 = fma(df, df, s2);
-      }
-      v = tab(sqrt(s2));
-    }
-    A[e] = v;
-  }
+constexpr int kDenseThreads = 256;
+
+template <typename T>
+struct DenseRootArgs {
+  const T* points;
+  long long n0;
+  int d;
+  TableBuffers tb;
+  double* A;          // n0 x n0, row-major; the lower triangle ends as L
+  int mode;           // 0: out = L in, 1: out = L^-1 in, 2: *out_logdet = sum log L_ii
+  const T* in;        // (n0,), gathered through perm when perm is set
+  const int* perm;    // graph row -> user index, or null
+  T* out_graph;       // (n0,) graph order, or null
+  T* out_user;        // scattered through perm (or graph order without perm), or null
+  double* x;          // (n0,) FP64 scratch of the inverse
+  double* out_logdet;
+  DeviceStatus* st;
+  unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ unsigned int dense_ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
-// Factor the diagonal tile (p, p) in place. 256 threads as 16 x 16; for each column j the pivot is read by all,
-// the column below it divided by the pivot's square root, and each thread updates the 4 x 4 block of the tile
-// it owns (rows 4ty.., columns 4tx..) where j < m <= i.
-__global__ void __launch_bounds__(256) dense_potrf_tile_kernel(double* __restrict__ A, long long n, int p) {
-  __shared__ double t[kDenseTile][kDenseTile + 1];
+// Grid-wide barrier over gridDim.x resident blocks; false when a wait ran out (the caller then returns).
+__device__ __forceinline__ bool dense_grid_barrier(DeviceStatus* st, unsigned long long timeout_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_ok = 1;
+    const unsigned int g = dense_ld_acquire(&st->bar_gen);
+    __threadfence();
+    if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+      atomicExch(&st->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    } else {
+      const uint64_t t0 = global_timer_ns();
+      unsigned int backoff = 32;
+      for (unsigned int it = 0; dense_ld_acquire(&st->bar_gen) == g; ++it) {
+        __nanosleep(backoff);
+        if (backoff < 256) backoff <<= 1;
+        if (global_timer_ns() - t0 > timeout_ns || it >= (1u << 30)) {
+          atomicAdd(&st->timeouts, 1u);
+          report_error(st, GGP_ERR_TIMEOUT);
+          s_ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Shared memory of one block: the diagonal tile and two 64 x 32 panel slices for the trailing update.
+struct DenseSmem {
+  double Lp[kDenseTile][kDenseTile + 1];
+  double Ai[kDenseTile][33];
+  double Aj[kDenseTile][33];
+};
+
+// Load and factor the diagonal tile (p, p) into s.Lp (lower triangle, zeros above, identity past the end).
+__device__ __forceinline__ void dense_factor_diag(const double* __restrict__ A, long long n, int p, DenseSmem& s) {
   const long long o = (long long)p * kDenseTile;
   const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  for (int r = ty; r < nb; r += 16)
-    for (int c = tx; c < nb; c += 16) t[r][c] = A[(o + r) * n + o + c];
+  for (int e = tid; e < kDenseTile * kDenseTile; e += kDenseThreads) {
+    const int r = e >> 6, c = e & 63;
+    s.Lp[r][c] = (r < nb && c < nb && c <= r) ? A[(o + r) * n + o + c] : (r == c ? 1.0 : 0.0);
+  }
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
-    const double djj = sqrt(t[j][j]);
+    const double djj = sqrt(s.Lp[j][j]);
     __syncthreads();  // every thread has read the pivot before it is overwritten
     if (tid < nb) {
-      if (tid > j) t[tid][j] /= djj;
-      else if (tid == j) t[j][j] = djj;
+      if (tid > j) s.Lp[tid][j] /= djj;
+      else if (tid == j) s.Lp[j][j] = djj;
     }
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int i = ty * 4 + u;
       if (i > j && i < nb) {
-        const double lij = t[i][j];
+        const double lij = s.Lp[i][j];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
           const int m = tx * 4 + v;
-          if (m > j && m <= i) t[i][m] -= lij * t[m][j];
+          if (m > j && m <= i) s.Lp[i][m] -= lij * s.Lp[m][j];
         }
       }
     }
     __syncthreads();  // the next pivot was just updated
   }
-  for (int r = ty; r < nb; r += 16)
-    for (int c = tx; c < nb; c += 16) A[(o + r) * n + o + c] = (c <= r) ? t[r][c] : 0.0;
 }
 
-// Panel solve: tile rows below p, X L_pp^T = A_ip; one block per tile row, one thread per matrix row, the row's
-// unknowns in registers (compile-time indices).
-__global__ void __launch_bounds__(kDenseTile) dense_trsm_kernel(double* __restrict__ A, long long n, int p) {
-  __shared__ double Lp[kDenseTile][kDenseTile + 1];
+// Tile row ti (below panel p): L_ip = A_ip L_pp^-T in place, one thread per matrix row (threads 0..63).
+__device__ __forceinline__ void dense_solve_row_tile(double* __restrict__ A, long long n, int p, int ti,
+                                                     const DenseSmem& s) {
   const long long o = (long long)p * kDenseTile;
   const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, j = e - i * nb;
-    Lp[i][j] = A[(o + i) * n + o + j];
-  }
-  __syncthreads();
-  const long long r = o + (long long)(blockIdx.x + 1) * kDenseTile + threadIdx.x;
-  if (r >= n) return;
+  const long long r = (long long)ti * kDenseTile + threadIdx.x;
+  if (threadIdx.x >= kDenseTile || r >= n) return;
   double x[kDenseTile];
   double* row = A + r * n + o;
 #pragma unroll
   for (int j = 0; j < kDenseTile; ++j) {
     if (j < nb) {
-      double s = row[j];
+      double v = row[j];
 #pragma unroll
-      for (int m = 0; m < j; ++m) s = fma(-x[m], Lp[j][m], s);
-      x[j] = s / Lp[j][j];
+      for (int m = 0; m < j; ++m) v = fma(-x[m], s.Lp[j][m], v);
+      x[j] = v / s.Lp[j][j];
     }
   }
 #pragma unroll
@@ -102,35 +142,31 @@ __global__ void __launch_bounds__(kDenseTile) dense_trsm_kernel(double* __restri
     if (j < nb) row[j] = x[j];
 }
 
-// Trailing update of lower tiles (i, j), p < j <= i: A_ij -= A_ip A_jp^T. One block (16 x 16 threads,
-// 4 x 4 outputs each) per tile; blockIdx.x enumerates the lower-triangular tile pairs; the panel is
-// staged 32 columns at a time.
-__global__ void __launch_bounds__(256) dense_update_kernel(double* __restrict__ A, long long n, int p, int nt) {
+// Trailing tile (ti, tj), ti >= tj > p: A_ij -= L_ip L_jp^T (16 x 16 threads, 4 x 4 outputs each).
+__device__ __forceinline__ void dense_update_tile(double* __restrict__ A, long long n, int p, int ti, int tj,
+                                                  DenseSmem& s) {
   constexpr int KC = 32;
-  __shared__ double Ai[kDenseTile][KC + 1];
-  __shared__ double Aj[kDenseTile][KC + 1];
-  // decode lower-triangular pair index -> (ti, tj) over tiles p+1..nt-1
-  const int e = blockIdx.x;
-  int ti = 0;
-  while ((ti + 1) * (ti + 2) / 2 <= e) ++ti;
-  const int tj = e - ti * (ti + 1) / 2;
-  const long long oi = (long long)(p + 1 + ti) * kDenseTile, oj = (long long)(p + 1 + tj) * kDenseTile;
+  const long long oi = (long long)ti * kDenseTile, oj = (long long)tj * kDenseTile;
   const long long op = (long long)p * kDenseTile;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double acc[4][4] = {};
   for (int k0 = 0; k0 < kDenseTile; k0 += KC) {
     __syncthreads();
-    for (int q = threadIdx.x; q < kDenseTile * KC; q += blockDim.x) {
+    for (int q = threadIdx.x; q < kDenseTile * KC; q += kDenseThreads) {
       const int r = q / KC, c = q - r * KC;
-      Ai[r][c] = (oi + r < n) ? A[(oi + r) * n + op + k0 + c] : 0.0;
-      Aj[r][c] = (oj + r < n) ? A[(oj + r) * n + op + k0 + c] : 0.0;
+      const bool kin = op + k0 + c < n;
+      s.Ai[r][c] = (oi + r < n && kin) ? A[(oi + r) * n + op + k0 + c] : 0.0;
+      s.Aj[r][c] = (oj + r < n && kin) ? A[(oj + r) * n + op + k0 + c] : 0.0;
     }
     __syncthreads();
 #pragma unroll 8
     for (int m = 0; m < KC; ++m) {
       double a[4], b[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) { a[u] = Ai[ty * 4 + u][m]; b[u] = Aj[tx * 4 + u][m]; }
+      for (int u = 0; u < 4; ++u) {
+        a[u] = s.Ai[ty * 4 + u][m];
+        b[u] = s.Aj[tx * 4 + u][m];
+      }
 #pragma unroll
       for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -149,96 +185,157 @@ __global__ void __launch_bounds__(256) dense_update_kernel(double* __restrict__ 
   }
 }
 
-// out_graph[i] = sum_{j <= i} L[i][j] xi[perm ? perm[j] : j]; optional scatter to user order.
-template <typename T>
-__global__ void dense_matvec_kernel(const double* __restrict__ L, long long n0, const T* __restrict__ xi,
-                                    const int* __restrict__ perm, T* __restrict__ out_graph, T* __restrict__ out_user,
-                                    DeviceStatus* st) {
-  const int lane = threadIdx.x & 31;
-  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long i = w; i < n0; i += nw) {
-    double s = 0.0;
-    for (long long j = lane; j <= i; j += 32) s = fma(L[i * n0 + j], (double)xi[perm ? perm[j] : j], s);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-      const T v = canonical((T)s);
-      if (v != v) atomicOr(&st->nan_seen, 1u);
-      if (out_graph) out_graph[i] = v;
-      if (out_user) out_user[perm ? perm[i] : i] = v;
-    }
-  }
+// Lower-triangular tile index t -> (ti, tj), tj <= ti.
+__device__ __forceinline__ void tile_pair(int t, int& ti, int& tj) {
+  ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+  while (ti * (ti + 1) / 2 > t) --ti;
+  tj = t - ti * (ti + 1) / 2;
 }
 
-// Forward substitution L x = v in one block of 1024 threads, 32 rows at a time: all warps form the dot
-// products against the already-solved prefix, then warp 0 finishes the 32 x 32 triangle.
 template <typename T>
-__global__ void __launch_bounds__(1024) dense_trsv_kernel(const double* __restrict__ L, long long n0,
-                                                          const T* __restrict__ v, const int* __restrict__ perm,
-                                                          double* __restrict__ x, T* __restrict__ out_graph,
-                                                          T* __restrict__ out_user, DeviceStatus* st) {
+__global__ void __launch_bounds__(kDenseThreads) dense_root_kernel(DenseRootArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char dense_smem[];
+  DenseSmem& s = *reinterpret_cast<DenseSmem*>(dense_smem);
+  const long long n = a.n0;
+  const int nt = (int)((n + kDenseTile - 1) / kDenseTile);
+  // covariance, lower tiles only (every later read stays in the lower triangle)
+  {
+    const TableView<double> tab = global_table_view<double>(a.tb);
+    const double c0 = a.tb.desc->c0;
+    const int ntiles = nt * (nt + 1) / 2;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      int ti, tj;
+      tile_pair(t, ti, tj);
+      for (int e = threadIdx.x; e < kDenseTile * kDenseTile; e += kDenseThreads) {
+        const long long i = (long long)ti * kDenseTile + (e >> 6), j = (long long)tj * kDenseTile + (e & 63);
+        if (i >= n || j >= n || j > i) continue;
+        double v = c0;
+        if (i != j) {
+          double s2 = 0.0;
+          for (int c = 0; c < a.d; ++c) {
+            const double df = (double)a.points[i * a.d + c] - (double)a.points[j * a.d + c];
+            s2 = fma(df, df, s2);
+          }
+          v = tab(sqrt(s2));
+        }
+        a.A[i * n + j] = v;
+      }
+    }
+  }
+  if (!dense_grid_barrier(a.st, a.timeout_ns)) return;
+  for (int p = 0; p < nt; ++p) {
+    const int below = nt - p - 1;
+    if ((int)blockIdx.x < (below > 0 ? below : 1)) {
+      dense_factor_diag(a.A, n, p, s);
+      for (int t = blockIdx.x; t < below; t += gridDim.x) dense_solve_row_tile(a.A, n, p, p + 1 + t, s);
+    }
+    if (!dense_grid_barrier(a.st, a.timeout_ns)) return;
+    if (blockIdx.x == 0) {  // the factored diagonal tile (still in this block's shared memory)
+      const long long o = (long long)p * kDenseTile;
+      const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
+      for (int e = threadIdx.x; e < kDenseTile * kDenseTile; e += kDenseThreads) {
+        const int r = e >> 6, c = e & 63;
+        if (r < nb && c <= r) a.A[(o + r) * n + o + c] = s.Lp[r][c];
+      }
+    }
+    const int tiles = below * (below + 1) / 2;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+      int ti, tj;
+      tile_pair(t, ti, tj);
+      dense_update_tile(a.A, n, p, p + 1 + ti, p + 1 + tj, s);
+    }
+    if (!dense_grid_barrier(a.st, a.timeout_ns)) return;
+  }
+  const double* L = a.A;
+  if (a.mode == 0) {  // out = L in: one warp per row
+    const int lane = threadIdx.x & 31;
+    const long long w = ((long long)blockIdx.x * kDenseThreads + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * kDenseThreads) >> 5;
+    for (long long i = w; i < n; i += nw) {
+      double acc = 0.0;
+      for (long long j = lane; j <= i; j += 32) acc = fma(L[i * n + j], (double)a.in[a.perm ? a.perm[j] : j], acc);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) {
+        const T v = canonical((T)acc);
+        if (v != v) atomicOr(&a.st->nan_seen, 1u);
+        if (a.out_graph) a.out_graph[i] = v;
+        if (a.out_user) a.out_user[a.perm ? a.perm[i] : i] = v;
+      }
+    }
+    return;
+  }
+  if (blockIdx.x != 0) return;
+  if (a.mode == 2) {
+    __shared__ double s_ld[kDenseThreads / 32];
+    double acc = 0.0;
+    for (long long i = threadIdx.x; i < n; i += kDenseThreads) acc += log(L[i * n + i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s_ld[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kDenseThreads / 32; ++w) t += s_ld[w];
+      *a.out_logdet = t;
+    }
+    return;
+  }
+  // forward substitution L x = v, 32 rows at a time: the warps form the dot products against the solved prefix,
+  // then warp 0 finishes the 32 x 32 triangle
   __shared__ double s_rhs[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (long long b0 = 0; b0 < n0; b0 += 32) {
-    const long long i = b0 + warp;
-    if (i < n0) {
-      double s = 0.0;
-      for (long long j = lane; j < b0; j += 32) s = fma(L[i * n0 + j], x[j], s);
+  for (long long b0 = 0; b0 < n; b0 += 32) {
+    for (int rr = warp; rr < 32; rr += kDenseThreads / 32) {
+      const long long i = b0 + rr;
+      if (i >= n) continue;
+      double acc = 0.0;
+      for (long long j = lane; j < b0; j += 32) acc = fma(L[i * n + j], a.x[j], acc);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) s_rhs[warp] = (double)v[perm ? perm[i] : i] - s;
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) s_rhs[rr] = (double)a.in[a.perm ? a.perm[i] : i] - acc;
     }
     __syncthreads();
     if (warp == 0) {
       const long long r = b0 + lane;
-      double rhs = (r < n0) ? s_rhs[lane] : 0.0;
+      double rhs = (r < n) ? s_rhs[lane] : 0.0;
       double xr = 0.0;
-      for (int j = 0; j < 32 && b0 + j < n0; ++j) {
-        const double lrj = (r < n0 && j < lane) ? L[r * n0 + b0 + j] : 0.0;
-        const double xj = __shfl_sync(0xffffffffu, (lane == j) ? rhs / L[r * n0 + r] : 0.0, j);
+      for (int j = 0; j < 32 && b0 + j < n; ++j) {
+        const double lrj = (r < n && j < lane) ? L[r * n + b0 + j] : 0.0;
+        const double xj = __shfl_sync(0xffffffffu, (lane == j) ? rhs / L[r * n + r] : 0.0, j);
         if (lane == j) xr = xj;
         rhs = fma(-lrj, xj, rhs);
       }
-      if (r < n0) {
-        x[r] = xr;
+      if (r < n) {
+        a.x[r] = xr;
         const T o = canonical((T)xr);
-        if (o != o) atomicOr(&st->nan_seen, 1u);
-        if (out_graph) out_graph[r] = o;
-        if (out_user) out_user[perm ? perm[r] : r] = o;
+        if (o != o) atomicOr(&a.st->nan_seen, 1u);
+        if (a.out_graph) a.out_graph[r] = o;
+        if (a.out_user) a.out_user[a.perm ? a.perm[r] : r] = o;
       }
     }
     __syncthreads();
   }
 }
 
-__global__ void dense_logdet_kernel(const double* __restrict__ L, long long n0, double* __restrict__ out) {
-  __shared__ double s[32];
-  double acc = 0.0;
-  for (long long i = threadIdx.x; i < n0; i += blockDim.x) acc += log(L[i * n0 + i]);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
-    *out = t;
-  }
-}
-
-// Factor A (n0 x n0, row-major, holding the covariance) in place.
-inline cudaError_t dense_cholesky(double* A, long long n0, cudaStream_t s) {
-  const int nt = (int)((n0 + kDenseTile - 1) / kDenseTile);
-  for (int p = 0; p < nt; ++p) {
-    (ggp::count_launch(), dense_potrf_tile_kernel<<<1, 256, 0, s>>>(A, n0, p));
-    const int below = nt - p - 1;
-    if (below > 0) {
-      (ggp::count_launch(), dense_trsm_kernel<<<below, kDenseTile, 0, s>>>(A, n0, p));
-      (ggp::count_launch(), dense_update_kernel<<<below * (below + 1) / 2, 256, 0, s>>>(A, n0, p, nt));
-    }
-  }
-  return cudaGetLastError();
+// Launch the cooperative dense root: as many blocks as the largest panel phase has tiles, at most what the device
+// keeps resident.
+template <typename T>
+cudaError_t launch_dense_root(const DenseRootArgs<T>& args, cudaStream_t s) {
+  auto kern = dense_root_kernel<T>;
+  const size_t smem = sizeof(DenseSmem);
+  cudaError_t e = allow_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const long long nt = (args.n0 + kDenseTile - 1) / kDenseTile;
+  long long want = (nt - 1) * nt / 2;
+  if (want < nt) want = nt;
+  const int cap = persistent_grid(kern, kDenseThreads, smem, 0);
+  const int grid = (int)(want < cap ? want : cap);
+  void* params[] = {const_cast<DenseRootArgs<T>*>(&args)};
+  ggp::count_launch();
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(kDenseThreads), params, smem,
+                                     s);
 }
 
 }  // namespace ggp

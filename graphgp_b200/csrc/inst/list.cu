@@ -1,0 +1,50 @@
+// Launchers of the FP64 list pass (refine_list.cuh), one instantiation per padded neighbour count and dimension.
+#include "../refine_list.cuh"
+
+namespace ggp {
+
+namespace {
+
+template <int K, int D>
+cudaError_t launch_list_kd(const RefineParams<float>& p, bool logdet, int nb, cudaStream_t s) {
+  const int warps = list_warps<K, D>(nb);
+  if (warps < 1) return cudaErrorInvalidConfiguration;
+  RefineParams<float> q = p;
+  q.table_smem = (int)((table_smem_bytes<double>(nb) + 255) / 256 * 256);
+  const int block = warps * 32;
+  const size_t smem = q.table_smem + sizeof(double) * 8 * QuadSmem<K, D>::kPerPoint * (size_t)warps;
+  auto kern = logdet ? refine_list_kernel<K, D, true> : refine_list_kernel<K, D, false>;
+  cudaError_t e = allow_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const int grid = persistent_grid(kern, block, smem, logdet ? kMaxPartials : 0);
+  (ggp::count_launch(), kern<<<grid, block, smem, s>>>(q));
+  return cudaGetLastError();
+}
+
+template <int K>
+int list_warps_d(int d, int nb) {
+  return d == 2 ? list_warps<K, 2>(nb) : list_warps<K, 3>(nb);
+}
+
+}  // namespace
+
+bool list_supported(int k, int d, int nb) {
+  if (k < 1 || k > kListMaxK || (d != 2 && d != 3)) return false;
+  const int K = list_k(k);
+  const int w = K == 8 ? list_warps_d<8>(d, nb) : (K == 16 ? list_warps_d<16>(d, nb) : list_warps_d<20>(d, nb));
+  return w >= 1;
+}
+
+cudaError_t launch_list(const RefineParams<float>& p, bool logdet, int nb, cudaStream_t s) {
+  const int K = list_k(p.k);
+  if (p.d == 2) {
+    if (K == 8) return launch_list_kd<8, 2>(p, logdet, nb, s);
+    if (K == 16) return launch_list_kd<16, 2>(p, logdet, nb, s);
+    return launch_list_kd<20, 2>(p, logdet, nb, s);
+  }
+  if (K == 8) return launch_list_kd<8, 3>(p, logdet, nb, s);
+  if (K == 16) return launch_list_kd<16, 3>(p, logdet, nb, s);
+  return launch_list_kd<20, 3>(p, logdet, nb, s);
+}
+
+}  // namespace ggp

@@ -1,12 +1,16 @@
 // Host launchers and C-ABI entry points for refinement, the dense root and whole-graph generate /
 // inverse / logdet.
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "dense.cuh"
 #include "refine_generic.cuh"
 #include "workspace.cuh"
 #include "refine_launch.cuh"
+#include "refine_list.cuh"
+#include "refine_tpp.cuh"
 #include "vjp.cuh"
 #include "vjp_quad.cuh"
 
@@ -110,9 +114,43 @@ inline int grid_for(long long n, int block = 256) {
 // ------------------------------------------------------------------------------------------------
 // kernel dispatch on (k, d); the register-resident instantiations live in inst_*.cu
 // ------------------------------------------------------------------------------------------------
+// The one-thread-per-point FP32 kernel (refine_tpp.cuh) takes k <= 16, d in {2, 3}, tables whose brackets fit
+// in shared memory, and neighbour rows aligned for its vector loads. GGP_REFINE_KERNEL=quad in the environment
+// selects the four-lanes-per-point kernels instead (comparison runs and tests of both paths).
+inline bool tpp_disabled() {
+  static const bool off = [] {
+    const char* v = getenv("GGP_REFINE_KERNEL");
+    return v && strcmp(v, "quad") == 0;
+  }();
+  return off;
+}
+
+template <int D>
+cudaError_t dispatch_tpp(const RefineParams<float>& p, int kind, int nb, int max_blocks, cudaStream_t s, bool* done) {
+  *done = false;
+  const int k = p.k;
+  if (k > kTppMaxK || tpp_disabled()) return cudaSuccess;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if ((long)tpp_table_smem(nb) > (long)optin - kSmemHeadroom) return cudaSuccess;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p.nbrs);
+  *done = true;
+  if (k == 16 && (a & 15) == 0) return launch_tpp<16, D, false>(p, kind, nb, max_blocks, s);
+  if (k == 10 && (a & 7) == 0) return launch_tpp<10, D, false>(p, kind, nb, max_blocks, s);
+  if (k == 8 && (a & 15) == 0) return launch_tpp<8, D, false>(p, kind, nb, max_blocks, s);
+  if (k <= 8) return launch_tpp<8, D, true>(p, kind, nb, max_blocks, s);
+  return launch_tpp<16, D, true>(p, kind, nb, max_blocks, s);
+}
+
 template <typename T, int D>
 cudaError_t dispatch_k(const RefineParams<T>& p, int kind, int nb, int max_blocks, cudaStream_t s) {
   const int k = p.k;
+  if constexpr (sizeof(T) == 4) {
+    bool done = false;
+    cudaError_t e = dispatch_tpp<D>(p, kind, nb, max_blocks, s, &done);
+    if (done) return e;
+  }
   switch (k) {
     case 8: return launch_fast<T, 8, D, false>(p, kind, nb, max_blocks, s);
     case 10: return launch_fast<T, 10, D, false>(p, kind, nb, max_blocks, s);
@@ -145,15 +183,30 @@ cudaError_t dispatch(const RefineParams<T>& p, int kind, int nb, int max_blocks,
 // common argument checks
 // ------------------------------------------------------------------------------------------------
 inline int check_refine_args(const void* points, long long n, int d, const void* nbrs, int k, const void* offsets,
-                             int n_offsets, const void* bins, const void* vals, int nb) {
+                             int n_offsets, const void* bins, const void* vals, int nb, int tbytes = 4) {
   if (!points || !bins || !vals) return GGP_ERR_INVALID;
   if (n < 1 || d < 1 || k < 1 || nb < 2 || n_offsets < 1) return GGP_ERR_INVALID;
   if (n_offsets > 1 && (!nbrs || !offsets)) return GGP_ERR_INVALID;
+  // the kernels load int32 ids and, for d = 2, both coordinates of a point at once
+  if (reinterpret_cast<uintptr_t>(points) & (uintptr_t)((d == 2 ? 2 : 1) * tbytes - 1)) return GGP_ERR_INVALID;
+  if ((reinterpret_cast<uintptr_t>(nbrs) & 3) || (reinterpret_cast<uintptr_t>(offsets) & 3)) return GGP_ERR_INVALID;
   if (nb > kMaxBins) return GGP_ERR_UNSUPPORTED;
   if (n > 0x7fffffffLL) return GGP_ERR_UNSUPPORTED;
   if (generic_smem_bytes(k, d) > 227 * 1024 && !(d == 2 || d == 3)) return GGP_ERR_UNSUPPORTED;
   if (k > 32 && generic_smem_bytes(k, d) > 227 * 1024) return GGP_ERR_UNSUPPORTED;
   return GGP_OK;
+}
+
+// Diagnostic builds (-DGGP_DEVICE_CHECKS) synchronise after each stage of a call and name the stage whose work
+// failed; release builds compile this away.
+inline void stage_done(const char* where, cudaStream_t s) {
+#ifdef GGP_DEVICE_CHECKS
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) fprintf(stderr, "graphgp_b200: stage %s failed: %s\n", where, cudaGetErrorString(e));
+#else
+  (void)where;
+  (void)s;
+#endif
 }
 
 inline int cuda_status(cudaError_t e) {
@@ -198,7 +251,21 @@ int run_cond(RefineParams<T> p, int mode, int nb, cudaStream_t s) {
   p.mode = mode;
   if (p.n_batches < 1 || p.n == p.n0) return GGP_OK;
   // generate waits batch on batch: -1 lets the launcher cap its width for the block size it picks
-  return cuda_status(dispatch<T>(p, kCond, nb, mode == kGenerate ? -1 : 0, s));
+  cudaError_t e = dispatch<T>(p, kCond, nb, mode == kGenerate ? -1 : 0, s);
+  stage_done("refinement", s);
+  if constexpr (sizeof(T) == 4) {
+    if (e == cudaSuccess && mode == kInverse && p.fb_rows) e = launch_list(p, false, nb, s);
+    stage_done("list pass", s);
+  }
+  return cuda_status(e);
+}
+
+// The row list of the FP64 second pass, when this FP32 inverse / logdet can use it (else null: points below tau
+// are re-conditioned in place).
+template <typename T>
+int* list_rows(const Workspace& ws, int k, int d, int nb) {
+  if constexpr (sizeof(T) == 4) return (ws.fb_rows && list_supported(k, d, nb)) ? ws.fb_rows : nullptr;
+  return nullptr;
 }
 
 template <typename T>
@@ -206,6 +273,9 @@ int run_logdet(RefineParams<T> p, int nb, double* out, const double* add, cudaSt
   cudaMemsetAsync(p.logdet_partials, 0, sizeof(double) * kMaxPartials, s);
   if (p.n > p.n0) {
     cudaError_t e = dispatch<T>(p, kLogdet, nb, kMaxPartials, s);
+    if constexpr (sizeof(T) == 4) {
+      if (e == cudaSuccess && p.fb_rows) e = launch_list(p, true, nb, s);
+    }
     if (e != cudaSuccess) return cuda_status(e);
   }
   (ggp::count_launch(), sum_partials_kernel<<<1, 1024, 0, s>>>(p.logdet_partials, kMaxPartials, add, out));
@@ -238,7 +308,8 @@ __global__ void init_refine_values_kernel(T* __restrict__ values, const T* __res
   }
 }
 
-// Dense root on points[0:n0) (graph order). mode 0: out = L xi; 1: out = L^-1 v; 2: logdet.
+// Dense root on points[0:n0) (graph order). mode 0: out = L xi; 1: out = L^-1 v; 2: logdet. One cooperative
+// launch (dense_root_kernel) covers the covariance, the factorisation and the solve.
 template <typename T>
 int dense_root(const Workspace& ws, const T* points, long long n0, int d, int mode, const T* in, const int* perm,
                T* out_graph, T* out_user, double* out_logdet, cudaStream_t s) {
@@ -246,17 +317,22 @@ int dense_root(const Workspace& ws, const T* points, long long n0, int d, int mo
     if (mode == 2) { cudaMemsetAsync(out_logdet, 0, sizeof(double), s); }
     return cuda_status(cudaGetLastError());
   }
-  (ggp::count_launch(), dense_cov_kernel<T><<<grid_for(n0 * n0), 256, 0, s>>>(points, n0, d, nullptr, ws.table, ws.dense));
-  cudaError_t e = dense_cholesky(ws.dense, n0, s);
-  if (e != cudaSuccess) return cuda_status(e);
-  if (mode == 0) {
-    (ggp::count_launch(), dense_matvec_kernel<T><<<grid_for(n0 * 32), 256, 0, s>>>(ws.dense, n0, in, perm, out_graph, out_user, ws.status));
-  } else if (mode == 1) {
-    (ggp::count_launch(), dense_trsv_kernel<T><<<1, 1024, 0, s>>>(ws.dense, n0, in, perm, ws.dense_x, out_graph, out_user, ws.status));
-  } else {
-    (ggp::count_launch(), dense_logdet_kernel<<<1, 1024, 0, s>>>(ws.dense, n0, out_logdet));
-  }
-  return cuda_status(cudaGetLastError());
+  DenseRootArgs<T> a{};
+  a.points = points;
+  a.n0 = n0;
+  a.d = d;
+  a.tb = ws.table;
+  a.A = ws.dense;
+  a.mode = mode;
+  a.in = in;
+  a.perm = perm;
+  a.out_graph = out_graph;
+  a.out_user = out_user;
+  a.x = ws.dense_x;
+  a.out_logdet = out_logdet;
+  a.st = ws.status;
+  a.timeout_ns = 10000000000ull;
+  return cuda_status(launch_dense_root<T>(a, s));
 }
 
 }  // namespace ggp
@@ -272,7 +348,7 @@ template <typename T>
 int refine_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k, const int32_t* offsets,
                 int n_offsets, const T* bins, const T* vals, int nb, const T* init, const T* xi, T* out, double tau,
                 uint64_t timeout_ns, void* wsp, size_t ws_bytes, cudaStream_t s) {
-  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !out || !init || (n > n0 && !xi)) return GGP_ERR_INVALID;
   Workspace ws;
@@ -290,7 +366,7 @@ template <typename T>
 int refine_inv_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k, const int32_t* offsets,
                     int n_offsets, const T* bins, const T* vals, int nb, const T* values, T* out_init, T* out_xi,
                     double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
-  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !values || !out_init || (n > n0 && !out_xi)) return GGP_ERR_INVALID;
   if (tau < 0) tau = GGP_DEFAULT_TAU_INVERSE;
@@ -302,21 +378,23 @@ int refine_inv_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
   p.values = const_cast<T*>(values);
   p.xi_out = out_xi;
+  p.fb_rows = list_rows<T>(ws, k, d, nb);
   return run_cond<T>(p, kInverse, nb, s);
 }
 
 template <typename T>
 int refine_logdet_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                        const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, double* out,
-                       double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
-  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+                       double tau, void* wsp, size_t ws_bytes, cudaStream_t s, bool fb_list = true) {
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !out) return GGP_ERR_INVALID;
   Workspace ws;
-  rc = carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  rc = carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws, fb_list);
   if (rc) return rc;
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
+  p.fb_rows = list_rows<T>(ws, k, d, nb);
   return run_logdet<T>(p, nb, out, nullptr, s);
 }
 
@@ -338,7 +416,7 @@ template <typename T>
 int generate_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                   const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* xi, T* out,
                   double tau, uint64_t timeout_ns, void* wsp, size_t ws_bytes, cudaStream_t s) {
-  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !xi || !out) return GGP_ERR_INVALID;
   Workspace ws;
@@ -369,7 +447,7 @@ template <typename T>
 int generate_inv_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                       const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* values,
                       T* out_xi, double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
-  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !values || !out_xi) return GGP_ERR_INVALID;
   if (tau < 0) tau = GGP_DEFAULT_TAU_INVERSE;
@@ -377,15 +455,19 @@ int generate_inv_impl(const T* points, const int32_t* perm, int64_t n, int d, in
   rc = carve_workspace(GGP_OP_GENERATE_INV, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
   if (rc) return rc;
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  stage_done("prologue", s);
   T* vg = (T*)ws.values_graph;
   (ggp::count_launch(), gather_kernel<T><<<grid_for(n), 256, 0, s>>>(values, perm, vg, n));  // values in graph order
+  stage_done("gather", s);
   // dense part: xi[:n0] = L^-1 v[:n0] (refine.py:186-195), gathered from / scattered to user order
   if ((rc = dense_root<T>(ws, points, n0, d, 1, values, perm, nullptr, out_xi, nullptr, s))) return rc;
+  stage_done("dense root", s);
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
   p.values = vg;
   p.perm = perm;
   p.out_user = perm ? out_xi : nullptr;
   p.xi_out = perm ? nullptr : out_xi + n0;
+  p.fb_rows = list_rows<T>(ws, k, d, nb);
   if ((rc = run_cond<T>(p, kInverse, nb, s))) return rc;
   (ggp::count_launch(), poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out_xi, n, ws.status));
   return cuda_status(cudaGetLastError());
@@ -395,7 +477,7 @@ template <typename T>
 int generate_logdet_impl(const T* points, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                          const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, double* out,
                          double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
-  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !out) return GGP_ERR_INVALID;
   Workspace ws;
@@ -405,6 +487,7 @@ int generate_logdet_impl(const T* points, int64_t n, int d, int64_t n0, const in
   // dense logdet (refine.py:243-248) lands in dense_x[0]; the refined sum adds it (refine.py:238-240)
   if ((rc = dense_root<T>(ws, points, n0, d, 2, nullptr, nullptr, nullptr, nullptr, ws.dense_x, s))) return rc;
   RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, 0);
+  p.fb_rows = list_rows<T>(ws, k, d, nb);
   return run_logdet<T>(p, nb, out, ws.dense_x, s);
 }
 
@@ -566,7 +649,7 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
                         const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* xi,
                         const T* values, const T* g_values, double g_logdet, T* out_grad_xi, double* out_grad_vals,
                         double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
-  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb);
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !xi || !g_values || !out_grad_xi || !out_grad_vals) return GGP_ERR_INVALID;
   if (k > kVjpMaxK || d > kVjpMaxD) return GGP_ERR_UNSUPPORTED;
@@ -778,11 +861,11 @@ extern "C" int ggp_refine_logdet_f32_noalloc(const float* points, int64_t n, int
     return GGP_ERR_UNSUPPORTED;
   }
   Workspace need;
-  carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, n_bins, n_offsets, 4, nullptr, 0, &need);
+  carve_workspace(GGP_OP_REFINE_LOGDET, n, d, n0, k, n_bins, n_offsets, 4, nullptr, 0, &need, false);
   if (need.total > kNoAllocScratchBytes) return GGP_ERR_UNSUPPORTED;  // unreachable under the limits above
   void* scratch = nullptr;
   rc = noalloc_scratch(&scratch);
   if (rc) return rc;
   return refine_logdet_impl<float>(points, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
-                                   out_logdet, tau, scratch, kNoAllocScratchBytes, GGP_STREAM(stream));
+                                   out_logdet, tau, scratch, kNoAllocScratchBytes, GGP_STREAM(stream), false);
 }

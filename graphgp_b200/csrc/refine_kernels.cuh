@@ -31,6 +31,8 @@ struct RefineParams {
   TableBuffers tb;
   DeviceStatus* status;
   double tau;               // FP64 re-conditioning threshold on the pivot ratio (0 disables)
+  int* fb_rows;             // inverse / logdet: rows below tau are listed here (count in status->listed) for the
+                            // FP64 second pass instead of being re-conditioned in place; or null
   int table_smem;           // bytes of dynamic shared memory taken by the staged table (256-aligned)
   unsigned long long timeout_ns;
 };
@@ -42,13 +44,14 @@ struct RefineParams {
 __host__ __device__ __forceinline__ int chunk_rows(long long) { return 8; }
 
 // Block cap for a dependency-ordered launch over rows [n0, n) in n_batches batches: dataflow_width() warps per
-// average chunk of a batch (at least 8 warps), as blocks of warps_per_block; 0 = no cap.
-inline int dataflow_blocks(long long n, long long n0, int n_batches, int warps_per_block) {
+// average chunk of a batch (at least 8 warps), as blocks of warps_per_block; 0 = no cap. chunks_per_warp: chunks a
+// warp works on at once (4 for the one-thread-per-point kernel).
+inline int dataflow_blocks(long long n, long long n0, int n_batches, int warps_per_block, int chunks_per_warp = 1) {
   const double w = dataflow_width();
   if (!(w > 0.0) || n_batches < 1 || n <= n0) return 0;
   const double avg = double(n - n0) / n_batches;
   const double chunks = std::ceil(avg / chunk_rows((long long)avg));
-  double warps = std::ceil(w * chunks);
+  double warps = std::ceil(w * chunks / chunks_per_warp);
   if (warps < 8) warps = 8;
   const double blocks = std::ceil(warps / warps_per_block);
   return blocks > 1e9 ? 0 : (int)blocks;
@@ -103,5 +106,18 @@ __device__ __forceinline__ void load_point(const T* __restrict__ points, long lo
 
 template <typename T>
 __device__ __forceinline__ void atomic_flag(unsigned int* f) { atomicOr(f, 1u); }
+
+// Append a refined row to the FP64 second pass's list (inverse / logdet). The list holds n - n0 rows, one per
+// refined row; a slot past the end (a row listed twice) is refused and reported instead of written.
+template <typename T>
+__device__ __forceinline__ void list_row(const RefineParams<T>& p, long long row) {
+  const unsigned int slot = atomicAdd(&p.status->listed, 1u);
+  if ((long long)slot < p.n - p.n0) {
+    p.fb_rows[slot] = (int)row;
+    atomicAdd(&p.status->fallback_count, 1u);
+  } else {
+    report_error(p.status, GGP_ERR_INVALID);
+  }
+}
 
 }  // namespace ggp

@@ -384,6 +384,7 @@ __device__ __forceinline__ void quad_pairs(const T* __restrict__ crd, T* __restr
   int i = 1, j = g;
   while (j >= i) { j -= i; ++i; }
   for (int pp = g; pp < SM::kPairs; pp += kQuad) {
+    if (!GGP_CHECK(i <= K && j >= 0 && j < i, 302, i, j)) break;
     T a = T(0);
     if (!(PAD && ((i < K && i >= kk) || j >= kk))) {
       T pi[D], pj[D];
@@ -523,15 +524,21 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
       __syncwarp();  // the scratch is reused by the next sub-iteration
       mr = quad_min(mr);
       const bool fb = sizeof(T) == 4 && active && !(mr >= (T)p.tau);  // quad-uniform
+      // inverse / logdet with a row list: the FP64 second pass (refine_list.cuh) finishes this point
+      const bool defer = fb && !gen && p.fb_rows != nullptr;
       double w64[K];
       double vd64 = 0.0;
-      if (fb && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
+      if (fb && !defer && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
+      // every lane runs quad_mean (its quad sum is a full-warp shuffle), deferred points included
       T mean = T(0);
       if (!LOGDET) mean = quad_mean<T, K>(p, gen, may_wait, ids, g, wmine, ok);
       int okv = ok ? 1 : 0;  // quad-wide AND, both shuffles executed by every lane
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
-      if (active && g == 0) quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
+      if (active && g == 0) {
+        if (defer) list_row(p, row);
+        else quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
+      }
     }
   }
   if (LOGDET) {

@@ -12,6 +12,7 @@
 // result exact for any sorted table.
 #pragma once
 
+#include "checks.cuh"
 #include "common.cuh"
 
 namespace ggp {
@@ -223,6 +224,7 @@ struct TableView {
       c = (int)(cl < 0 ? 0 : (cl >= n_hint ? n_hint - 1 : cl));
     }
     int j = hint[c];
+    if (!GGP_CHECK(j >= 0 && j <= last, 301, j, c)) j = 0;
     Bracket<T> e = br[j];
     if (max_steps <= 2) {
 #pragma unroll

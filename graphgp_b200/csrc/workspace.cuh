@@ -16,6 +16,7 @@ struct Workspace {
   void* values_graph = nullptr;     // n values (generate / generate_inv / vjp)
   double* dense = nullptr;          // n0 * n0 doubles (dense root factor)
   double* dense_x = nullptr;        // n0 doubles
+  int* fb_rows = nullptr;           // FP32 inverse / logdet: rows left to the FP64 second pass (n - n0 ints)
   void* extra = nullptr;            // op-specific
   size_t extra_bytes = 0;
   size_t total = 0;
@@ -36,8 +37,10 @@ struct Carver {
 size_t graph_extra_bytes(int op, long long n, int d, long long n0, int k, int tbytes);
 size_t vjp_extra_bytes(long long n, long long n0, int k, int nb, int tbytes);
 
+// fb_list: carve the row list of the FP64 second pass (FP32 inverse / logdet); the no-allocation log-determinant
+// runs without it, re-conditioning in place.
 inline int carve_workspace(int op, long long n, int d, long long n0, int k, int nb, int n_offsets, int tbytes,
-                           void* base, size_t bytes, Workspace* ws) {
+                           void* base, size_t bytes, Workspace* ws, bool fb_list = true) {
   Carver c(base);
   Workspace w;
   w.status = (DeviceStatus*)c.take(sizeof(DeviceStatus));
@@ -63,6 +66,9 @@ inline int carve_workspace(int op, long long n, int d, long long n0, int k, int 
     w.extra = c.take(extra);
     w.extra_bytes = extra;
   }
+  const bool listed = op == GGP_OP_REFINE_INV || op == GGP_OP_REFINE_LOGDET || op == GGP_OP_GENERATE_INV ||
+                      op == GGP_OP_GENERATE_LOGDET;
+  if (fb_list && listed && tbytes == 4 && n > n0) w.fb_rows = (int*)c.take(sizeof(int) * (size_t)(n - n0));
   w.total = c.off;
   if (ws) *ws = w;
   if (base && bytes < w.total) return GGP_ERR_WORKSPACE;

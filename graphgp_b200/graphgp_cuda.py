@@ -20,8 +20,17 @@ import torch
 from . import _lib
 
 DEFAULT_TAU = 1e-5
-"""FP32 points whose smallest Cholesky pivot ratio (Schur complement / prior variance) falls below this
-threshold are re-conditioned in FP64."""
+"""generate and log-determinant: FP32 points whose smallest Cholesky pivot ratio (Schur complement / prior variance)
+falls below this threshold are re-conditioned in FP64 (``GGP_DEFAULT_TAU``)."""
+
+DEFAULT_TAU_INVERSE = 3e-3
+"""inverse: the same rule with a larger threshold (``GGP_DEFAULT_TAU_INVERSE``). xi = (v - mean) / std divides the
+FP32 rounding of the mean by std, so the inverse needs FP64 wherever a pivot ratio is small; for k <= 20 and
+d in {2, 3} an FP64 second pass finishes those points. ``tau=None`` picks each operation's default."""
+
+
+def _tau(tau):
+    return -1.0 if tau is None else float(tau)
 
 _tls = threading.local()
 
@@ -224,7 +233,7 @@ def _refine_common(points, neighbors, offsets):
     return points, sfx, nb, n, d, n0, k, offs
 
 
-def refine(points, neighbors, offsets, cov_bins, cov_vals, initial_values, xi, *, tau=DEFAULT_TAU, timeout_ns=0):
+def refine(points, neighbors, offsets, cov_bins, cov_vals, initial_values, xi, *, tau=None, timeout_ns=0):
     """``graphgp_cuda.refine`` (refine.py:119-121): values (N,) in graph order."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
@@ -239,7 +248,7 @@ def refine(points, neighbors, offsets, cov_bins, cov_vals, initial_values, xi, *
     lib = _lib.load()
     if sfx == "f32":
         rc = lib.ggp_refine_f32(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins), _ptr(vals),
-                                len(bins), _ptr(init), _ptr(xi), _ptr(out), float(tau), int(timeout_ns), _ptr(ws),
+                                len(bins), _ptr(init), _ptr(xi), _ptr(out), _tau(tau), int(timeout_ns), _ptr(ws),
                                 ws.numel(), _stream())
     else:
         rc = lib.ggp_refine_f64(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins), _ptr(vals),
@@ -249,7 +258,7 @@ def refine(points, neighbors, offsets, cov_bins, cov_vals, initial_values, xi, *
     return out
 
 
-def refine_inv(points, neighbors, offsets, cov_bins, cov_vals, values, *, tau=DEFAULT_TAU):
+def refine_inv(points, neighbors, offsets, cov_bins, cov_vals, values, *, tau=None):
     """``graphgp_cuda.refine_inv`` (refine.py:216-218) -> (initial_values (n0,), xi (N - n0,))."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
@@ -262,7 +271,7 @@ def refine_inv(points, neighbors, offsets, cov_bins, cov_vals, values, *, tau=DE
     lib = _lib.load()
     if sfx == "f32":
         rc = lib.ggp_refine_inv_f32(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
-                                    _ptr(vals), len(bins), _ptr(values), _ptr(init), _ptr(xi), float(tau), _ptr(ws),
+                                    _ptr(vals), len(bins), _ptr(values), _ptr(init), _ptr(xi), _tau(tau), _ptr(ws),
                                     ws.numel(), _stream())
     else:
         rc = lib.ggp_refine_inv_f64(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
@@ -272,7 +281,7 @@ def refine_inv(points, neighbors, offsets, cov_bins, cov_vals, values, *, tau=DE
     return init, xi
 
 
-def refine_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=DEFAULT_TAU):
+def refine_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=None):
     """``graphgp_cuda.refine_logdet`` (refine.py:265): sum of log std, FP64 accumulation (0-d float64 tensor)."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
@@ -281,7 +290,7 @@ def refine_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=DEFAULT
     lib = _lib.load()
     if sfx == "f32":
         rc = lib.ggp_refine_logdet_f32(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
-                                       _ptr(vals), len(bins), _ptr(out), float(tau), _ptr(ws), ws.numel(), _stream())
+                                       _ptr(vals), len(bins), _ptr(out), _tau(tau), _ptr(ws), ws.numel(), _stream())
     else:
         rc = lib.ggp_refine_logdet_f64(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
                                        _ptr(vals), len(bins), _ptr(out), _ptr(ws), ws.numel(), _stream())
@@ -312,7 +321,7 @@ def dense(mode, points, cov_bins, cov_vals, x=None):
     return out if m < 2 else ld
 
 
-def generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau=DEFAULT_TAU, timeout_ns=0):
+def generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau=None, timeout_ns=0):
     """Whole ``generate`` (reference refine.py:21-56) in one device call: xi (N,) in the original order ->
     values (N,) in the original order; ``indices`` may be None."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
@@ -326,7 +335,7 @@ def generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau
     lib = _lib.load()
     if sfx == "f32":
         rc = lib.ggp_generate_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
-                                  _ptr(vals), len(bins), _ptr(xi), _ptr(out), float(tau), int(timeout_ns), _ptr(ws),
+                                  _ptr(vals), len(bins), _ptr(xi), _ptr(out), _tau(tau), int(timeout_ns), _ptr(ws),
                                   ws.numel(), _stream())
     else:
         rc = lib.ggp_generate_f64(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
@@ -336,7 +345,7 @@ def generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau
     return out
 
 
-def generate_inv(points, indices, neighbors, offsets, cov_bins, cov_vals, values, *, tau=DEFAULT_TAU):
+def generate_inv(points, indices, neighbors, offsets, cov_bins, cov_vals, values, *, tau=None):
     """Whole ``generate_inv`` (reference refine.py:162-183) in one device call."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
@@ -349,7 +358,7 @@ def generate_inv(points, indices, neighbors, offsets, cov_bins, cov_vals, values
     lib = _lib.load()
     if sfx == "f32":
         rc = lib.ggp_generate_inv_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
-                                      _ptr(bins), _ptr(vals), len(bins), _ptr(values), _ptr(out), float(tau), _ptr(ws),
+                                      _ptr(bins), _ptr(vals), len(bins), _ptr(values), _ptr(out), _tau(tau), _ptr(ws),
                                       ws.numel(), _stream())
     else:
         rc = lib.ggp_generate_inv_f64(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
@@ -359,7 +368,7 @@ def generate_inv(points, indices, neighbors, offsets, cov_bins, cov_vals, values
     return out
 
 
-def generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=DEFAULT_TAU):
+def generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=None):
     """Whole ``generate_logdet`` (reference refine.py:234-240): dense + refined, 0-d float64 tensor."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
@@ -368,7 +377,7 @@ def generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=DEFAU
     lib = _lib.load()
     if sfx == "f32":
         rc = lib.ggp_generate_logdet_f32(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
-                                         _ptr(vals), len(bins), _ptr(out), float(tau), _ptr(ws), ws.numel(), _stream())
+                                         _ptr(vals), len(bins), _ptr(out), _tau(tau), _ptr(ws), ws.numel(), _stream())
     else:
         rc = lib.ggp_generate_logdet_f64(_ptr(points), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs), _ptr(bins),
                                          _ptr(vals), len(bins), _ptr(out), _ptr(ws), ws.numel(), _stream())
@@ -377,7 +386,7 @@ def generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=DEFAU
 
 
 def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_values, g_logdet=0.0, *,
-                 tau=DEFAULT_TAU, values=None):
+                 tau=None, values=None):
     """Adjoint of generate (+ g_logdet * generate_logdet): returns (grad_xi (N,), grad_cov_vals (n_bins,) f64).
 
     ``values``: generate's output for these same inputs, if the caller has it (the primal output a custom_vjp
@@ -401,7 +410,7 @@ def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_
         rc = lib.ggp_generate_vjp_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
                                       _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(values), _ptr(g),
                                       float(g_logdet), _ptr(gx),
-                                      _ptr(gv), float(tau), _ptr(ws), ws.numel(), _stream())
+                                      _ptr(gv), _tau(tau), _ptr(ws), ws.numel(), _stream())
     else:
         rc = lib.ggp_generate_vjp_f64(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
                                       _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(values), _ptr(g),
@@ -414,7 +423,7 @@ def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_
 _REQUEST_OPS = {"generate": 0, "inverse": 1, "logdet": 2}
 
 
-def request(op, points, n0, k, cov_bins, cov_vals, payload=None, *, tau=DEFAULT_TAU):
+def request(op, points, n0, k, cov_bins, cov_vals, payload=None, *, tau=None):
     """Graph build plus one operation in a single native call (``ggp_request_*``): op "generate" (payload = xi)
     or "inverse" (payload = values) -> (N,) tensor in the caller's order; "logdet" -> 0-d float64 tensor. Builds
     the same graph as ``build_graph(points, n0=n0, k=k)``; the call waits on the current stream once."""
@@ -445,7 +454,7 @@ def request(op, points, n0, k, cov_bins, cov_vals, payload=None, *, tau=DEFAULT_
     _tls.last_ws = buf
     if sfx == "f32":
         rc = lib.ggp_request_f32(m, _ptr(points), n, d, int(n0), int(k), _ptr(bins), _ptr(vals), len(bins),
-                                 _ptr(payload if m < 2 else None), _ptr(out), _ptr(ld), float(tau), _ptr(buf),
+                                 _ptr(payload if m < 2 else None), _ptr(out), _ptr(ld), _tau(tau), _ptr(buf),
                                  buf.numel(), _stream())
     else:
         rc = lib.ggp_request_f64(m, _ptr(points), n, d, int(n0), int(k), _ptr(bins), _ptr(vals), len(bins),

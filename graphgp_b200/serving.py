@@ -202,7 +202,7 @@ class Engine:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.slots = int(slots)
         self.budget = int(hbm_budget)
-        self.tau = gc.DEFAULT_TAU if tau is None else tau
+        self.tau = tau  # None: each operation's default threshold
         self.fused = fused  # requests with nothing resident: one native call (ggp_request_*) or separate calls
         self.dtype = dtype or torch.float32
         if self.dtype not in (torch.float32, torch.float64):

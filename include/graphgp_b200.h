@@ -146,10 +146,13 @@ int ggp_build_graph_f64(const double* points, int64_t n, int d, int64_t n0, int 
 /* offsets[0] = n0, offsets[n_offsets-1] = n; n0 = n - rows(neighbors) (refine.py:111).              */
 /* `tau` (f32 functions only): a point whose smallest pivot ratio (Schur complement / prior variance) */
 /* falls below tau is re-conditioned in FP64; 0 disables it, a negative value selects the default of  */
-/* the operation: GGP_DEFAULT_TAU for generate and log-determinant, GGP_DEFAULT_TAU_INVERSE for the   */
-/* inverse. The inverse needs the larger threshold because xi = (v - mean) / std divides the FP32     */
-/* rounding of the mean by std: with smooth kernels most pivot ratios sit near the jitter (1e-4), and */
-/* a pure FP32 inverse then misses 1e-4 relative error (FP32 NumPy gets 4e-4 on such graphs).         */
+/* the operation: GGP_DEFAULT_TAU for generate and the log-determinant, GGP_DEFAULT_TAU_INVERSE for   */
+/* the inverse. The inverse needs the larger threshold: xi = (v - mean) / std divides the FP32        */
+/* rounding of the mean by std, and with smooth kernels or dense points most pivot ratios sit a       */
+/* little above the jitter, where a pure FP32 inverse misses 1e-4 relative error (FP32 NumPy gets    */
+/* 3e-4 to 5e-4 on such graphs against FP64 on the same inputs). For k <= 20 and d in {2, 3} the      */
+/* inverse and log-determinant finish such points in an FP64 second pass over a row list kept in the  */
+/* workspace; other shapes re-condition them in place.                                               */
 /* `timeout_ns` bounds every wait of a point on a neighbour value (0 = default 10 s; values above     */
 /* GGP_MAX_TIMEOUT_NS are clamped to it).                                                           */
 /* ---------------------------------------------------------------------------------------------- */
@@ -299,6 +302,16 @@ int ggp_request_f64(int op, const double* points, int64_t n, int d, int64_t n0, 
 /* ---------------------------------------------------------------------------------------------- */
 int ggp_wait_probe(uint64_t timeout_ns, int* out_code, void* workspace, size_t workspace_bytes,
                    ggp_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Arithmetic peak probe (measurement only; no counterpart in the reference): enqueues `blocks` blocks */
+/* of 256 threads that each run 8 independent FMA chains for `iters` rounds. kind 0 = FP32 (fma.rn.f32),  */
+/* 1 = packed FP32 (fma.rn.f32x2), 2 = FP64. *out_flops (host) receives the floating-point operations    */
+/* enqueued (2 per FMA); time the call with events on `stream`. `sink` is a device buffer of at least  */
+/* 2048 bytes that the kernel writes only to keep its work from being optimised away.                 */
+/* ---------------------------------------------------------------------------------------------- */
+int ggp_fma_probe(int kind, int blocks, int iters, double* out_flops, void* sink, size_t sink_bytes,
+                  ggp_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -32,3 +32,11 @@ def rbf_table(scale=0.3, r_min=1e-4, r_max=10.0, n_bins=1001, jitter=1e-4):
 
 def matern32_table(cutoff=0.05, r_min=1e-6, r_max=4.0, n_bins=2049, jitter=1e-5):
     return ox.matern_kernel(p=1, variance=1.0, cutoff=cutoff, r_min=r_min, r_max=r_max, n_bins=n_bins, jitter=jitter)
+
+
+def as_inputs(cov, dtype):
+    """The table as a kernel of that dtype receives it: rounded to `dtype`, held in float64 for the oracle. FP32
+    results are compared with the FP64 oracle on these same inputs, so that the error measured is the FP32
+    arithmetic's, not the rounding of the caller's table (which alone moves a smooth-kernel inverse by ~2e-4)."""
+    bins, vals = cov
+    return (np.asarray(bins).astype(dtype).astype(np.float64), np.asarray(vals).astype(dtype).astype(np.float64))

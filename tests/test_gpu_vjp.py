@@ -11,7 +11,7 @@ import pytest
 from oracle import adjoint as oa
 
 from conftest import rel_err
-from helpers import oracle_graph, matern32_table, rbf_table
+from helpers import as_inputs, oracle_graph, matern32_table, rbf_table
 
 pytestmark = pytest.mark.gpu
 
@@ -55,7 +55,7 @@ def test_vjp_f32_vs_oracle(cuda_device, n, d, n0, k, tab, gl):
     from graphgp_b200 import graphgp_cuda as gc
 
     pts, g = oracle_graph(n, d, n0, k)
-    bins, vals = _table(tab)
+    bins, vals = as_inputs(_table(tab), np.float32)
     rng = np.random.default_rng(n + k + 1)
     xi, gv = rng.standard_normal(n), rng.standard_normal(n)
     rx, rv = oa.generate_vjp(g, (bins, vals), xi, gv, gl)
@@ -114,9 +114,12 @@ def test_vjp_differentiation_workload_shape(cuda_device):
     y = orf.generate(g, (bins, vals), rng.standard_normal(n)) + 0.01 * rng.standard_normal(n)
     xi = rng.standard_normal(n)
     v = orf.generate(g, (bins, vals), xi)
-    rx, rv = oa.generate_vjp(g, (bins, vals), xi, v - y, 1.0)
+    refs = {torch.float64: oa.generate_vjp(g, (bins, vals), xi, v - y, 1.0)}
+    c32 = as_inputs((bins, vals), np.float32)  # the FP64 oracle on the inputs the FP32 kernels receive
+    refs[torch.float32] = oa.generate_vjp(g, c32, xi, orf.generate(g, c32, xi) - y, 1.0)
     args = (_t(g.indices, cuda_device), _t(g.neighbors, cuda_device), g.offsets)
     for dt, tol_x, tol_v in ((torch.float64, 1e-8, 1e-8), (torch.float32, 1e-4, 1e-3)):
+        rx, rv = refs[dt]
         P = _t(g.points, cuda_device, dt)
         B, V = _t(bins, cuda_device, dt), _t(vals, cuda_device, dt)
         X = _t(xi, cuda_device, dt)
@@ -140,8 +143,9 @@ def test_vjp_general_kernel_vs_oracle(cuda_device, n, d, n0, k, tab, gl):
     bins, vals = _table(tab)
     rng = np.random.default_rng(n + 3 * k)
     xi, gv = rng.standard_normal(n), rng.standard_normal(n)
-    rx, rv = oa.generate_vjp(g, (bins, vals), xi, gv, gl)
     for dt, tol_x, tol_v in ((torch.float64, 1e-8, 1e-8), (torch.float32, 1e-4, 1e-3)):
+        rx, rv = oa.generate_vjp(g, as_inputs((bins, vals), np.float32 if dt == torch.float32 else np.float64), xi,
+                                 gv, gl)
         gx, gvals = gc.generate_vjp(_t(g.points, cuda_device, dt), _t(g.indices, cuda_device),
                                     _t(g.neighbors, cuda_device), g.offsets, _t(bins, cuda_device, dt),
                                     _t(vals, cuda_device, dt), _t(xi, cuda_device, dt), _t(gv, cuda_device, dt), gl)

@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from helpers import oracle_graph, matern32_table
+from helpers import as_inputs, oracle_graph, matern32_table
 from oracle import refine as orf
 
 pytestmark = pytest.mark.gpu
@@ -79,7 +79,7 @@ def test_noalloc_logdet_matches_workspace_version_twice(cuda_device, n, d, n0, k
     second = _logdet_noalloc(lib, args, cuda_device)
     for got in (first, second):
         assert abs(got - ref) <= TOL32 * abs(ref)
-    oracle = orf.refine_logdet(g.points, g.neighbors, g.offsets, cov)
+    oracle = orf.refine_logdet(g.points, g.neighbors, g.offsets, as_inputs(cov, np.float32))
     assert abs(second - oracle) <= TOL32 * abs(oracle)
 
 
