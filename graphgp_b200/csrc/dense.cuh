@@ -1,8 +1,8 @@
 // Dense root in FP64 on the GPU: the n0 x n0 covariance of the first n0 points, its Cholesky factor, and
 // L @ xi / L^-1 v / sum log L_ii (reference graphgp/refine.py:59-76, 186-195, 243-248).
 //
-// Blocked right-looking Cholesky on a row-major n0 x n0 matrix (lower triangle used; the upper triangle is never
-// written or read) with 64 x 64 tiles, all in one cooperative kernel: the whole dense root is one launch with no
+// Blocked right-looking Cholesky on a row-major n0 x n0 matrix (lower triangle used; the upper triangle is set to
+// zero) with 64 x 64 tiles, all in one cooperative kernel: the whole dense root is one launch with no
 // host round trip between panels. Per panel p:
 //   1. every block with a tile row below the panel (and block 0) factors the diagonal tile A_pp in shared memory
 //      (the same small factorisation, repeated, instead of a broadcast step); block t solves tile row p + 1 + t,
@@ -199,7 +199,8 @@ __global__ void __launch_bounds__(kDenseThreads) dense_root_kernel(DenseRootArgs
   DenseSmem& s = *reinterpret_cast<DenseSmem*>(dense_smem);
   const long long n = a.n0;
   const int nt = (int)((n + kDenseTile - 1) / kDenseTile);
-  // covariance, lower tiles only (every later read stays in the lower triangle)
+  // covariance in the lower triangle; the upper triangle is set to zero, so that the factor left in A is L itself
+  // (readers that take whole rows or transpose the matrix see zeros above the diagonal)
   {
     const TableView<double> tab = global_table_view<double>(a.tb);
     const double c0 = a.tb.desc->c0;
@@ -209,7 +210,12 @@ __global__ void __launch_bounds__(kDenseThreads) dense_root_kernel(DenseRootArgs
       tile_pair(t, ti, tj);
       for (int e = threadIdx.x; e < kDenseTile * kDenseTile; e += kDenseThreads) {
         const long long i = (long long)ti * kDenseTile + (e >> 6), j = (long long)tj * kDenseTile + (e & 63);
-        if (i >= n || j >= n || j > i) continue;
+        if (i >= n || j >= n) continue;
+        if (ti != tj) a.A[j * n + i] = 0.0;  // the mirrored upper tile
+        if (j > i) {
+          a.A[i * n + j] = 0.0;
+          continue;
+        }
         double v = c0;
         if (i != j) {
           double s2 = 0.0;

@@ -19,7 +19,8 @@ def _graph(dev, dtype, n=300, d=2, n0=40, k=8):
     pts, g = oracle_graph(n, d, n0, k, seed=7)
     graph = gg.Graph(torch.as_tensor(g.points, device=dev, dtype=dtype), torch.as_tensor(g.neighbors, device=dev),
                      g.offsets, torch.as_tensor(g.indices, device=dev))
-    bins, vals = rbf_table(scale=0.6, n_bins=101)
+    # a 1,001-entry table: linear interpolation of a coarser RBF table is not positive definite at this jitter
+    bins, vals = rbf_table(scale=0.3, n_bins=1001, jitter=1e-3)
     return graph, torch.as_tensor(bins, device=dev, dtype=dtype), torch.as_tensor(vals, device=dev, dtype=dtype)
 
 
@@ -63,6 +64,7 @@ def test_backward_equals_adjoint_fp32(cuda_device):
     xi = torch.randn(n, generator=gen, device=cuda_device).requires_grad_(True)
     vals = V.clone().requires_grad_(True)
     v, ld = gg.generate_and_logdet(graph, (B, vals), xi)
+    assert bool(torch.isfinite(v).all()) and bool(torch.isfinite(ld))
     loss = 0.5 * torch.sum((v - y) ** 2) + ld
     loss.backward()
     with torch.no_grad():
