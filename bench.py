@@ -657,15 +657,15 @@ def serving(dev, n_requests):
     return summ
 
 
-REFINE_KERNEL = "refine_tpp_kernel<16,3,false,false> (one thread per point, generate mode)"
+REFINE_KERNEL = "refine_quad2_kernel<float,16,3,false,kOpGenerate> (four lanes per point, generate)"
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the refinement kernel "
-                  "(profiles/refine_tpp_generate_c2.md, bytes per refined point), scaled to this launch's refined points")
+                  "(profiles/refine_quad_generate_c2.md, bytes per refined point), scaled to this launch's refined points")
 
 
 def read_traffic(units):
     """DRAM bytes per refined point of the dominant kernel from the committed ncu summary, scaled to one
     launch; None when no capture has been summarised."""
-    path = os.path.join(ROOT, "profiles", "refine_tpp_generate_c2.md")
+    path = os.path.join(ROOT, "profiles", "refine_quad_generate_c2.md")
     try:
         for ln in open(path):
             if ln.startswith("dram_bytes_per_point:"):

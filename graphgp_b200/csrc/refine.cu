@@ -114,9 +114,13 @@ inline int grid_for(long long n, int block = 256) {
 // ------------------------------------------------------------------------------------------------
 // kernel dispatch on (k, d); the register-resident instantiations live in inst_*.cu
 // ------------------------------------------------------------------------------------------------
-// The one-thread-per-point FP32 kernel (refine_tpp.cuh) takes k <= 16, d in {2, 3}, tables whose brackets fit
-// in shared memory, and neighbour rows aligned for its vector loads. GGP_REFINE_KERNEL=quad in the environment
-// selects the four-lanes-per-point kernels instead (comparison runs and tests of both paths).
+// The one-thread-per-point FP32 kernel (refine_tpp.cuh) takes k <= 10, d in {2, 3}, tables whose brackets fit
+// in shared memory, and neighbour rows aligned for its vector loads. Measured on 4M points (ms, this kernel /
+// the four-lanes-per-point kernel): d = 2, k = 10 generate 1.56 / 1.92, log-determinant 0.78 / 1.59; d = 3, k = 8
+// generate 0.84 / 1.48, log-determinant 0.61 / 1.25; but d = 2, k = 16 generate 6.31 / 4.14 (at k = 16 a thread's
+// 153-entry triangle leaves 8 to 12 resident warps per SM, too few to hide its neighbour gathers, and 32 points
+// per warp lengthen the dependency chain of generate). GGP_REFINE_KERNEL=quad in the environment selects the
+// four-lanes-per-point kernels for every k (comparison runs and tests of both paths).
 inline bool tpp_disabled() {
   static const bool off = [] {
     const char* v = getenv("GGP_REFINE_KERNEL");
@@ -136,11 +140,10 @@ cudaError_t dispatch_tpp(const RefineParams<float>& p, int kind, int nb, int max
   if ((long)tpp_table_smem(nb) > (long)optin - kSmemHeadroom) return cudaSuccess;
   const uintptr_t a = reinterpret_cast<uintptr_t>(p.nbrs);
   *done = true;
-  if (k == 16 && (a & 15) == 0) return launch_tpp<16, D, false>(p, kind, nb, max_blocks, s);
   if (k == 10 && (a & 7) == 0) return launch_tpp<10, D, false>(p, kind, nb, max_blocks, s);
   if (k == 8 && (a & 15) == 0) return launch_tpp<8, D, false>(p, kind, nb, max_blocks, s);
   if (k <= 8) return launch_tpp<8, D, true>(p, kind, nb, max_blocks, s);
-  return launch_tpp<16, D, true>(p, kind, nb, max_blocks, s);
+  return launch_tpp<10, D, true>(p, kind, nb, max_blocks, s);
 }
 
 template <typename T, int D>

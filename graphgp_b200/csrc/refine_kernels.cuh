@@ -9,6 +9,9 @@ namespace ggp {
 
 enum RefineMode : int { kGenerate = 0, kInverse = 1 };
 
+// Compile-time operation of a refinement kernel instantiation.
+enum RefineOp : int { kOpGenerate = 0, kOpInverse = 1, kOpLogdet = 2 };
+
 template <typename T>
 struct RefineParams {
   const T* points;          // (n, d) graph order

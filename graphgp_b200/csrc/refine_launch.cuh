@@ -31,7 +31,9 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
     if (warps < 1) return launch_generic<T>(p, kind, max_blocks < 0 ? 0 : max_blocks, s);
     const int block = (int)warps * 32;
     const size_t smem = q.table_smem + per_warp * warps;
-    auto kern = (kind == kCond) ? refine_quad2_kernel<T, K, D, PAD, false> : refine_quad2_kernel<T, K, D, PAD, true>;
+    auto kern = (kind != kCond) ? refine_quad2_kernel<T, K, D, PAD, kOpLogdet>
+                : (p.mode == kGenerate ? refine_quad2_kernel<T, K, D, PAD, kOpGenerate>
+                                       : refine_quad2_kernel<T, K, D, PAD, kOpInverse>);
     cudaError_t e = allow_smem(kern, smem);
     if (e != cudaSuccess) return e;
     if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, block / 32);

@@ -468,8 +468,12 @@ __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g
   min_ratio = mr;
 }
 
-template <typename T, int K, int D, bool PAD, bool LOGDET>
+// MODE is the operation, fixed at compile time (kOpGenerate, kOpInverse, kOpLogdet): the generate kernel carries no
+// code of the inverse / logdet row list, whose mere presence in the finishing block slowed the dependency-ordered
+// generate twofold.
+template <typename T, int K, int D, bool PAD, int MODE>
 __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(RefineParams<T> p) {
+  constexpr bool LOGDET = MODE == kOpLogdet;
   constexpr int NT = QuadRows<K>::NT;
   using SM = QuadSmem<K, D>;
   extern __shared__ __align__(32) unsigned char smem[];
@@ -485,7 +489,7 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
   const int src0 = lane & ~(kQuad - 1);
   T* crd = scratch + q * SM::kPerPoint;                      // (K+1) x kPointStride
   T* tri = crd + (K + 1) * SM::kPointStride;                 // kPairs
-  const bool gen = !LOGDET && p.mode == kGenerate;
+  constexpr bool gen = MODE == kOpGenerate;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
@@ -525,7 +529,7 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
       mr = quad_min(mr);
       const bool fb = sizeof(T) == 4 && active && !(mr >= (T)p.tau);  // quad-uniform
       // inverse / logdet with a row list: the FP64 second pass (refine_list.cuh) finishes this point
-      const bool defer = fb && !gen && p.fb_rows != nullptr;
+      const bool defer = !gen && fb && p.fb_rows != nullptr;
       double w64[K];
       double vd64 = 0.0;
       if (fb && !defer && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
@@ -536,7 +540,7 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
       if (active && g == 0) {
-        if (defer) list_row(p, row);
+        if (defer) list_row(p, row);  // constant false in the generate instantiation
         else quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
       }
     }

@@ -1,4 +1,4 @@
-// Refinement with one thread per point, FP32, for k <= 16 (generate with dataflow across depth batches,
+// Refinement with one thread per point, FP32, for k <= 10 (generate with dataflow across depth batches,
 // inverse and log-determinant).
 //
 // Per point (reference graphgp/refine.py:130-135, 278-285): joint = [nbr_0 .. nbr_{k-1}, self]; K = cov(joint,
@@ -24,8 +24,8 @@
 
 namespace ggp {
 
-constexpr int kTppBlock = 128;  // threads per block (3 blocks per SM at up to 168 registers)
-constexpr int kTppMaxK = 16;
+constexpr int kTppBlock = 128;  // threads per block
+constexpr int kTppMaxK = 10;
 #ifndef GGP_TPP_MIN_BLOCKS
 #define GGP_TPP_MIN_BLOCKS 3
 #endif
@@ -99,10 +99,11 @@ __device__ __forceinline__ float tpp_distance(const float (&a)[D], const float (
   return s * rsqrtf(fmaxf(s, 1.17549435e-38f));
 }
 
-// Generate (mode kGenerate) / inverse (kInverse) / log-determinant (LOGDET). PAD: k < K, rows k..K-1 are inert
-// (covariance 0 off the diagonal, c0 on it).
-template <int K, int D, bool PAD, bool LOGDET>
+// MODE: kOpGenerate / kOpInverse / kOpLogdet, fixed at compile time (the generate instantiation carries no row-list
+// code). PAD: k < K, rows k..K-1 are inert (covariance 0 off the diagonal, c0 on it).
+template <int K, int D, bool PAD, int MODE>
 __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kernel(RefineParams<float> p) {
+  constexpr bool LOGDET = MODE == kOpLogdet;
   constexpr int NA = tri_at(K, K) + 1;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double s_part[kTppBlock / 32];
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
   const float inv_c0 = 1.f / c0;
   const int lane = threadIdx.x & 31;
   const int kk = p.k;
-  const bool gen = !LOGDET && p.mode == kGenerate;
+  constexpr bool gen = MODE == kOpGenerate;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
@@ -200,9 +201,11 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
     // FP64 re-conditioning below the pivot threshold: in place (generate, or no row list), or left to the FP64
     // list pass (inverse / logdet with p.fb_rows)
     const bool fb = !(mr >= (float)p.tau);
-    if (fb && !gen && p.fb_rows) {
-      list_row(p, row);
-      continue;
+    if constexpr (!gen) {
+      if (fb && p.fb_rows) {
+        list_row(p, row);
+        continue;
+      }
     }
     double w64[K];
     double vd = (double)var;
@@ -319,7 +322,7 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
   }
 }
 
-// Launcher (inst/tpp_*.cu): kind 0 = generate / inverse (p.mode), 1 = log-determinant.
+// Launcher (inst/tpp_*.cu): kind 0 = generate / inverse (by p.mode), 1 = log-determinant.
 template <int K, int D, bool PAD>
 cudaError_t launch_tpp(const RefineParams<float>& p, int kind, int nb, int max_blocks, cudaStream_t s);
 
@@ -327,7 +330,9 @@ cudaError_t launch_tpp(const RefineParams<float>& p, int kind, int nb, int max_b
 template <int K, int D, bool PAD>
 cudaError_t launch_tpp(const RefineParams<float>& p, int kind, int nb, int max_blocks, cudaStream_t s) {
   const size_t smem = tpp_table_smem(nb);
-  auto kern = kind == 1 ? refine_tpp_kernel<K, D, PAD, true> : refine_tpp_kernel<K, D, PAD, false>;
+  auto kern = kind == 1 ? refine_tpp_kernel<K, D, PAD, kOpLogdet>
+              : (p.mode == kGenerate ? refine_tpp_kernel<K, D, PAD, kOpGenerate>
+                                     : refine_tpp_kernel<K, D, PAD, kOpInverse>);
   cudaError_t e = allow_smem(kern, smem);
   if (e != cudaSuccess) return e;
   if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, kTppBlock / 32, 4);
