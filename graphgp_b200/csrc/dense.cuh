@@ -2,14 +2,14 @@
 // L @ xi / L^-1 v / sum log L_ii (reference graphgp/refine.py:59-76, 186-195, 243-248).
 //
 // Blocked right-looking Cholesky on a row-major n0 x n0 matrix (lower triangle used; the upper triangle is set to
-// zero) with 64 x 64 tiles, all in one cooperative kernel: the whole dense root is one launch with no
-// host round trip between panels. Per panel p:
-//   1. every block with a tile row below the panel (and block 0) factors the diagonal tile A_pp in shared memory
-//      (the same small factorisation, repeated, instead of a broadcast step); block t solves tile row p + 1 + t,
-//      L_ip = A_ip L_pp^-T, and writes it;
+// zero) with 64 x 64 tiles, all in one cooperative kernel: the whole dense root is one launch with no host round
+// trip between panels. Per panel p:
+//   1. block t factors the 128 x 64 stack [A_pp; A_{p+1+t,p}] in registers (every block repeats the small
+//      diagonal factorisation instead of waiting for a broadcast) and writes L_{p+1+t,p} = A_{p+1+t,p} L_pp^-T;
 //   2. grid barrier; block 0 writes L_pp; every block takes trailing tiles (i, j), p < j <= i, A_ij -= L_ip L_jp^T;
 //   3. grid barrier.
-// Two barriers per panel replace three kernel launches per panel. The barrier is a sense-reversing counter in the
+// For L^-1 v the right-hand side is factored as one more matrix row (the augmented factor's last row is
+// (L^-1 v)^T), so the inverse costs what the factorisation costs. The barrier is a sense-reversing counter in the
 // status block whose waits are bounded (a wait that runs out records GGP_ERR_TIMEOUT and ends the block); the
 // launch is cooperative, so every block is resident and the barrier always completes.
 #pragma once
@@ -78,109 +78,178 @@ __device__ __forceinline__ bool dense_grid_barrier(DeviceStatus* st, unsigned lo
   return s_ok != 0;
 }
 
-// Shared memory of one block: the diagonal tile and two 64 x 32 panel slices for the trailing update.
-struct DenseSmem {
-  double Lp[kDenseTile][kDenseTile + 1];
-  double Ai[kDenseTile][33];
-  double Aj[kDenseTile][33];
+// The factored matrix: n x n row-major in A (tile rows 0 .. nt - 1), and for the inverse one more row, the
+// right-hand side in graph order, in xrow (tile row nt, row 0). The Cholesky factor of [[K, b], [b^T, *]] has
+// (L^-1 b)^T as its last row, so the factorisation itself performs the forward substitution.
+struct DenseMatrix {
+  double* A;
+  long long n;
+  int nt;    // tile rows (and columns) of A
+  bool rhs;  // tile row nt holds the right-hand side
+  double* xrow;
+  // Row r of tile row ti, or null past the end of the matrix.
+  __device__ __forceinline__ double* row(int ti, int r) const {
+    if (ti < nt) {
+      const long long g = (long long)ti * kDenseTile + r;
+      return g < n ? A + g * n : nullptr;
+    }
+    return (rhs && ti == nt && r == 0) ? xrow : nullptr;
+  }
 };
 
-// Load and factor the diagonal tile (p, p) into s.Lp (lower triangle, zeros above, identity past the end).
-__device__ __forceinline__ void dense_factor_diag(const double* __restrict__ A, long long n, int p, DenseSmem& s) {
-  const long long o = (long long)p * kDenseTile;
-  const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  for (int e = tid; e < kDenseTile * kDenseTile; e += kDenseThreads) {
-    const int r = e >> 6, c = e & 63;
-    s.Lp[r][c] = (r < nb && c < nb && c <= r) ? A[(o + r) * n + o + c] : (r == c ? 1.0 : 0.0);
-  }
-  __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    const double djj = sqrt(s.Lp[j][j]);
-    __syncthreads();  // every thread has read the pivot before it is overwritten
-    if (tid < nb) {
-      if (tid > j) s.Lp[tid][j] /= djj;
-      else if (tid == j) s.Lp[j][j] = djj;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = ty * 4 + u;
-      if (i > j && i < nb) {
-        const double lij = s.Lp[i][j];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          const int m = tx * 4 + v;
-          if (m > j && m <= i) s.Lp[i][m] -= lij * s.Lp[m][j];
-        }
-      }
-    }
-    __syncthreads();  // the next pivot was just updated
-  }
-}
+// Shared memory of one block: the two operand tiles of a trailing update, stored k-major (element (row, k) of a
+// tile at [k][row]) so that a thread's four rows are two 16-byte loads, and the column buffers of the panel
+// factorisation.
+constexpr int kDenseLd = kDenseTile + 2;  // row stride of the k-major tiles (16-byte aligned, fewer write conflicts)
+struct DenseSmem {
+  double Ai[kDenseTile][kDenseLd];
+  double Aj[kDenseTile][kDenseLd];
+  double col[2][kDenseTile];  // column j of the Schur complement of the diagonal tile, alternating buffers
+};
 
-// Tile row ti (below panel p): L_ip = A_ip L_pp^-T in place, one thread per matrix row (threads 0..63).
-__device__ __forceinline__ void dense_solve_row_tile(double* __restrict__ A, long long n, int p, int ti,
-                                                     const DenseSmem& s) {
+// Registers of one panel row: thread q = threadIdx.x & 1 of panel row threadIdx.x >> 1 holds the columns
+// 4 s + 2 q and 4 s + 2 q + 1 (s = 0..15) of its row.
+struct DensePanelRow {
+  double2 v[kDenseTile / 4];
+};
+
+// Right-looking factorisation of the 128 x 64 stack [A_pp; A_ip]: panel rows 0..63 are the diagonal tile (p, p),
+// rows 64..127 the tile (ti, p) (none when ti < 0). Afterwards the registers hold L_pp in the first 64 rows (lower
+// triangle) and L_ip = A_ip L_pp^-T in the last 64. Column j of the current Schur complement of the diagonal tile
+// goes through shared memory, alternating between two buffers, so that each column costs one block barrier: after
+// it every row takes its entry a_rj, stores l_rj = a_rj / sqrt(a_jj) and subtracts (a_rj / a_jj) a_mj from its
+// entries m > j. Rows of the diagonal tile above the pivot are finished and take no update. Past the end of the
+// matrix the diagonal tile is the identity and the row tile is zero.
+__device__ __forceinline__ void dense_panel_factor(const DenseMatrix& M, int p, int ti, DenseSmem& s,
+                                                   DensePanelRow& R) {
+  const long long n = M.n;
   const long long o = (long long)p * kDenseTile;
   const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
-  const long long r = (long long)ti * kDenseTile + threadIdx.x;
-  if (threadIdx.x >= kDenseTile || r >= n) return;
-  double x[kDenseTile];
-  double* row = A + r * n + o;
+  const int pr = threadIdx.x >> 1, q = threadIdx.x & 1;
+  const bool diag = pr < kDenseTile;
+  const double* src = diag ? (pr < nb ? M.A + (o + pr) * n : nullptr) : (ti >= 0 ? M.row(ti, pr - kDenseTile) : nullptr);
+  const bool valid = src != nullptr;
+  if (valid) src += o;
+#pragma unroll
+  for (int k = 0; k < kDenseTile / 4; ++k) {
+    const int c0 = 4 * k + 2 * q;
+    double x = 0.0, y = 0.0;
+    if (valid) {
+      if (c0 < nb && (!diag || c0 <= pr)) x = src[c0];
+      if (c0 + 1 < nb && (!diag || c0 + 1 <= pr)) y = src[c0 + 1];
+    } else if (diag) {
+      x = (c0 == pr) ? 1.0 : 0.0;
+      y = (c0 + 1 == pr) ? 1.0 : 0.0;
+    }
+    R.v[k] = make_double2(x, y);
+  }
 #pragma unroll
   for (int j = 0; j < kDenseTile; ++j) {
-    if (j < nb) {
-      double v = row[j];
+    constexpr int kSlots = kDenseTile / 4;
+    const int js = j >> 2, jq = (j >> 1) & 1;
+    const bool je = (j & 1) != 0;
+    double* cj = s.col[j & 1];
+    const double mine = je ? R.v[js].y : R.v[js].x;
+    if (diag && q == jq) cj[pr] = mine;
+    __syncthreads();
+    const double other = __shfl_xor_sync(0xffffffffu, mine, 1);
+    const double arj = (q == jq) ? mine : other;
+    const double invd = rsqrt(cj[j]);
+    const double l = arj * invd;
+    const double f = (diag && pr < j) ? 0.0 : l * invd;
+    if (q == jq) {
+      if (je) R.v[js].y = l;
+      else R.v[js].x = l;
+    }
 #pragma unroll
-      for (int m = 0; m < j; ++m) v = fma(-x[m], s.Lp[j][m], v);
-      x[j] = v / s.Lp[j][j];
+    for (int k = js; k < kSlots; ++k) {
+      const int m0 = 4 * k + 2 * q;
+      const double2 cm = *reinterpret_cast<const double2*>(&cj[m0]);
+      if (m0 > j) R.v[k].x = fma(-f, cm.x, R.v[k].x);
+      if (m0 + 1 > j) R.v[k].y = fma(-f, cm.y, R.v[k].y);
     }
   }
-#pragma unroll
-  for (int j = 0; j < kDenseTile; ++j)
-    if (j < nb) row[j] = x[j];
 }
 
-// Trailing tile (ti, tj), ti >= tj > p: A_ij -= L_ip L_jp^T (16 x 16 threads, 4 x 4 outputs each).
-__device__ __forceinline__ void dense_update_tile(double* __restrict__ A, long long n, int p, int ti, int tj,
-                                                  DenseSmem& s) {
-  constexpr int KC = 32;
-  const long long oi = (long long)ti * kDenseTile, oj = (long long)tj * kDenseTile;
+// Store the factored panel rows: the row tile always, the diagonal tile (lower triangle) when diag_too.
+__device__ __forceinline__ void dense_panel_store(const DenseMatrix& M, int p, int ti, const DensePanelRow& R,
+                                                  bool diag_too) {
+  const long long n = M.n;
+  const long long o = (long long)p * kDenseTile;
+  const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
+  const int pr = threadIdx.x >> 1, q = threadIdx.x & 1;
+  const bool diag = pr < kDenseTile;
+  double* dst = diag ? ((diag_too && pr < nb) ? M.A + (o + pr) * n : nullptr)
+                     : (ti >= 0 ? M.row(ti, pr - kDenseTile) : nullptr);
+  if (dst == nullptr) return;
+  dst += o;
+#pragma unroll
+  for (int k = 0; k < kDenseTile / 4; ++k) {
+    const int c0 = 4 * k + 2 * q;
+    if (c0 < nb && (!diag || c0 <= pr)) dst[c0] = R.v[k].x;
+    if (c0 + 1 < nb && (!diag || c0 + 1 <= pr)) dst[c0 + 1] = R.v[k].y;
+  }
+}
+
+// Trailing tile (ti, tj), ti >= tj > p: A_ij -= L_ip L_jp^T (16 x 16 threads, 4 x 4 outputs each). Both 64 x 64
+// operands are loaded once (all loads in flight before the first store), k-major, into shared memory; the outputs'
+// current values are fetched while the products are formed.
+__device__ __forceinline__ void dense_update_tile(const DenseMatrix& M, int p, int ti, int tj, DenseSmem& s) {
+  constexpr int kPer = kDenseTile * kDenseTile / kDenseThreads;  // operand elements per thread and operand
+  const long long n = M.n;
+  const long long oj = (long long)tj * kDenseTile;
   const long long op = (long long)p * kDenseTile;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int c = threadIdx.x & (kDenseTile - 1), r0 = threadIdx.x / kDenseTile;
+  const bool kin = op + c < n;
+  double va[kPer], vb[kPer];
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int r = r0 + i * (kDenseThreads / kDenseTile);
+    const double* ri = M.row(ti, r);
+    const double* rj = M.row(tj, r);
+    va[i] = (ri && kin) ? ri[op + c] : 0.0;
+    vb[i] = (rj && kin) ? rj[op + c] : 0.0;
+  }
+  __syncthreads();  // the previous tile's reads of shared memory are done
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int r = r0 + i * (kDenseThreads / kDenseTile);
+    s.Ai[c][r] = va[i];
+    s.Aj[c][r] = vb[i];
+  }
+  double* dst[4];
+  double cur[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    dst[u] = M.row(ti, ty * 4 + u);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int cc = tx * 4 + v;
+      cur[u][v] = (dst[u] && oj + cc < n && (ti > tj || cc <= ty * 4 + u)) ? dst[u][oj + cc] : 0.0;
+    }
+  }
+  __syncthreads();
   double acc[4][4] = {};
-  for (int k0 = 0; k0 < kDenseTile; k0 += KC) {
-    __syncthreads();
-    for (int q = threadIdx.x; q < kDenseTile * KC; q += kDenseThreads) {
-      const int r = q / KC, c = q - r * KC;
-      const bool kin = op + k0 + c < n;
-      s.Ai[r][c] = (oi + r < n && kin) ? A[(oi + r) * n + op + k0 + c] : 0.0;
-      s.Aj[r][c] = (oj + r < n && kin) ? A[(oj + r) * n + op + k0 + c] : 0.0;
-    }
-    __syncthreads();
 #pragma unroll 8
-    for (int m = 0; m < KC; ++m) {
-      double a[4], b[4];
+  for (int m = 0; m < kDenseTile; ++m) {
+    const double2 a01 = *reinterpret_cast<const double2*>(&s.Ai[m][ty * 4]);
+    const double2 a23 = *reinterpret_cast<const double2*>(&s.Ai[m][ty * 4 + 2]);
+    const double2 b01 = *reinterpret_cast<const double2*>(&s.Aj[m][tx * 4]);
+    const double2 b23 = *reinterpret_cast<const double2*>(&s.Aj[m][tx * 4 + 2]);
+    const double a[4] = {a01.x, a01.y, a23.x, a23.y}, b[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        a[u] = s.Ai[ty * 4 + u][m];
-        b[u] = s.Aj[tx * 4 + u][m];
-      }
+    for (int u = 0; u < 4; ++u)
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
-    }
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
   }
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
-    const long long r = oi + ty * 4 + u;
-    if (r >= n) continue;
+    if (dst[u] == nullptr) continue;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-      const long long c = oj + tx * 4 + v;
-      if (c < n && c <= r) A[r * n + c] -= acc[u][v];
+      const int cc = tx * 4 + v;
+      if (oj + cc < n && (ti > tj || cc <= ty * 4 + u)) dst[u][oj + cc] = cur[u][v] - acc[u][v];
     }
   }
 }
@@ -193,12 +262,21 @@ __device__ __forceinline__ void tile_pair(int t, int& ti, int& tj) {
   tj = t - ti * (ti + 1) / 2;
 }
 
+// Number of trailing tiles after panel p: the lower triangle of tile rows and columns p + 1 .. nt - 1, plus, with
+// the right-hand-side tile row (ntr = nt + 1), the tiles (nt, p + 1 .. nt - 1).
+__device__ __host__ __forceinline__ int dense_trailing_tiles(int nt, int ntr, int p) {
+  const int bc = nt - p - 1;
+  return bc * (bc + 1) / 2 + (ntr > nt ? bc : 0);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kDenseThreads) dense_root_kernel(DenseRootArgs<T> a) {
   extern __shared__ __align__(16) unsigned char dense_smem[];
   DenseSmem& s = *reinterpret_cast<DenseSmem*>(dense_smem);
   const long long n = a.n0;
   const int nt = (int)((n + kDenseTile - 1) / kDenseTile);
+  const DenseMatrix M{a.A, n, nt, a.mode == 1, a.x};
+  const int ntr = nt + (M.rhs ? 1 : 0);
   // covariance in the lower triangle; the upper triangle is set to zero, so that the factor left in A is L itself
   // (readers that take whole rows or transpose the matrix see zeros above the diagonal)
   {
@@ -228,28 +306,37 @@ __global__ void __launch_bounds__(kDenseThreads) dense_root_kernel(DenseRootArgs
         a.A[i * n + j] = v;
       }
     }
+    if (a.mode == 1)  // the right-hand side, graph order, as row n
+      for (long long i = (long long)blockIdx.x * kDenseThreads + threadIdx.x; i < n;
+           i += (long long)gridDim.x * kDenseThreads)
+        a.x[i] = (double)a.in[a.perm ? a.perm[i] : i];
   }
   if (!dense_grid_barrier(a.st, a.timeout_ns)) return;
   for (int p = 0; p < nt; ++p) {
-    const int below = nt - p - 1;
-    if ((int)blockIdx.x < (below > 0 ? below : 1)) {
-      dense_factor_diag(a.A, n, p, s);
-      for (int t = blockIdx.x; t < below; t += gridDim.x) dense_solve_row_tile(a.A, n, p, p + 1 + t, s);
+    // 1. every block factors [A_pp; A_ip] for its tile row i (block 0 also when there is none) ...
+    const int below = ntr - p - 1;
+    const int rows = below > 0 ? below : 1;
+    DensePanelRow R;
+    for (int t = blockIdx.x; t < rows; t += gridDim.x) {
+      const int ti = below > 0 ? p + 1 + t : -1;
+      dense_panel_factor(M, p, ti, s, R);
+      dense_panel_store(M, p, ti, R, false);
     }
     if (!dense_grid_barrier(a.st, a.timeout_ns)) return;
-    if (blockIdx.x == 0) {  // the factored diagonal tile (still in this block's shared memory)
-      const long long o = (long long)p * kDenseTile;
-      const int nb = (int)((n - o) < kDenseTile ? (n - o) : kDenseTile);
-      for (int e = threadIdx.x; e < kDenseTile * kDenseTile; e += kDenseThreads) {
-        const int r = e >> 6, c = e & 63;
-        if (r < nb && c <= r) a.A[(o + r) * n + o + c] = s.Lp[r][c];
-      }
-    }
-    const int tiles = below * (below + 1) / 2;
+    // 2. ... then block 0 stores L_pp, still in its registers (every block has read A_pp by now), and the blocks
+    //    share the trailing update
+    if (blockIdx.x == 0) dense_panel_store(M, p, -1, R, true);
+    const int bc = nt - p - 1, tri = bc * (bc + 1) / 2;
+    const int tiles = dense_trailing_tiles(nt, ntr, p);
     for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
       int ti, tj;
-      tile_pair(t, ti, tj);
-      dense_update_tile(a.A, n, p, p + 1 + ti, p + 1 + tj, s);
+      if (t < tri) {
+        tile_pair(t, ti, tj);
+      } else {
+        ti = nt - p - 1;  // the right-hand-side tile row nt
+        tj = t - tri;
+      }
+      dense_update_tile(M, p, p + 1 + ti, p + 1 + tj, s);
     }
     if (!dense_grid_barrier(a.st, a.timeout_ns)) return;
   }
@@ -272,56 +359,28 @@ __global__ void __launch_bounds__(kDenseThreads) dense_root_kernel(DenseRootArgs
     }
     return;
   }
-  if (blockIdx.x != 0) return;
-  if (a.mode == 2) {
-    __shared__ double s_ld[kDenseThreads / 32];
-    double acc = 0.0;
-    for (long long i = threadIdx.x; i < n; i += kDenseThreads) acc += log(L[i * n + i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) s_ld[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < kDenseThreads / 32; ++w) t += s_ld[w];
-      *a.out_logdet = t;
+  if (a.mode == 1) {  // out = L^-1 in: the last row of the augmented factor
+    for (long long i = (long long)blockIdx.x * kDenseThreads + threadIdx.x; i < n;
+         i += (long long)gridDim.x * kDenseThreads) {
+      const T o = canonical((T)a.x[i]);
+      if (o != o) atomicOr(&a.st->nan_seen, 1u);
+      if (a.out_graph) a.out_graph[i] = o;
+      if (a.out_user) a.out_user[a.perm ? a.perm[i] : i] = o;
     }
     return;
   }
-  // forward substitution L x = v, 32 rows at a time: the warps form the dot products against the solved prefix,
-  // then warp 0 finishes the 32 x 32 triangle
-  __shared__ double s_rhs[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (long long b0 = 0; b0 < n; b0 += 32) {
-    for (int rr = warp; rr < 32; rr += kDenseThreads / 32) {
-      const long long i = b0 + rr;
-      if (i >= n) continue;
-      double acc = 0.0;
-      for (long long j = lane; j < b0; j += 32) acc = fma(L[i * n + j], a.x[j], acc);
+  if (blockIdx.x != 0) return;
+  __shared__ double s_ld[kDenseThreads / 32];
+  double acc = 0.0;
+  for (long long i = threadIdx.x; i < n; i += kDenseThreads) acc += log(L[i * n + i]);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) s_rhs[rr] = (double)a.in[a.perm ? a.perm[i] : i] - acc;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      const long long r = b0 + lane;
-      double rhs = (r < n) ? s_rhs[lane] : 0.0;
-      double xr = 0.0;
-      for (int j = 0; j < 32 && b0 + j < n; ++j) {
-        const double lrj = (r < n && j < lane) ? L[r * n + b0 + j] : 0.0;
-        const double xj = __shfl_sync(0xffffffffu, (lane == j) ? rhs / L[r * n + r] : 0.0, j);
-        if (lane == j) xr = xj;
-        rhs = fma(-lrj, xj, rhs);
-      }
-      if (r < n) {
-        a.x[r] = xr;
-        const T o = canonical((T)xr);
-        if (o != o) atomicOr(&a.st->nan_seen, 1u);
-        if (a.out_graph) a.out_graph[r] = o;
-        if (a.out_user) a.out_user[a.perm ? a.perm[r] : r] = o;
-      }
-    }
-    __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s_ld[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kDenseThreads / 32; ++w) t += s_ld[w];
+    *a.out_logdet = t;
   }
 }
 
@@ -334,8 +393,9 @@ cudaError_t launch_dense_root(const DenseRootArgs<T>& args, cudaStream_t s) {
   cudaError_t e = allow_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const long long nt = (args.n0 + kDenseTile - 1) / kDenseTile;
-  long long want = (nt - 1) * nt / 2;
-  if (want < nt) want = nt;
+  const long long ntr = nt + (args.mode == 1 ? 1 : 0);
+  long long want = dense_trailing_tiles((int)nt, (int)ntr, 0);
+  if (want < ntr) want = ntr;
   const int cap = persistent_grid(kern, kDenseThreads, smem, 0);
   const int grid = (int)(want < cap ? want : cap);
   void* params[] = {const_cast<DenseRootArgs<T>*>(&args)};

@@ -147,7 +147,7 @@ def test_dense_root_vs_oracle(cuda_device):
     from graphgp_b200 import graphgp_cuda as gc
 
     rng = np.random.default_rng(5)
-    for n0 in (1, 37, 64, 200, 1030):
+    for n0 in (1, 37, 63, 64, 65, 128, 129, 200, 1030):  # ragged and whole 64-row tiles
         pts = rng.standard_normal((n0, 3))
         bins, vals = ox.matern_kernel(p=1, variance=1.0, cutoff=1.0, r_min=1e-4, r_max=20, n_bins=1000, jitter=1e-5)
         tb, tv, tp = _t(bins, cuda_device), _t(vals, cuda_device), _t(pts, cuda_device)
