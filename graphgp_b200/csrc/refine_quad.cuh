@@ -367,37 +367,84 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
 // ------------------------------------------------------------------------------------------------
 template <int K, int D> struct QuadSmem {
   static constexpr int kPairs = K * (K + 1) / 2;             // rows 1..K, columns below the diagonal
-  static constexpr int kPointStride = (D <= 2 ? 2 : 4);     // coordinates per point slot
-  static constexpr int kPerPoint = (K + 1) * kPointStride + kPairs + 1;  // +1 staggers banks
+  static constexpr int kPointStride = (D <= 2 ? 2 : 4);     // coordinates per point slot (one vector load)
+  // a multiple of 4 elements (16-byte aligned point slots), and not of 8, so that the eight points of a warp
+  // start on different banks
+  static constexpr int kRaw = ((K + 1) * kPointStride + kPairs + 3) / 4 * 4;
+  static constexpr int kPerPoint = kRaw % 8 == 0 ? kRaw + 4 : kRaw;
 };
 
 // Block size of the two-phase kernel: its launch bound (FP32: 20 warps at up to 96 registers, one block per
 // SM; FP64: 8 warps); the launch uses fewer warps when the table leaves too little shared memory.
 template <typename T> struct Quad2Block { static constexpr int kMax = sizeof(T) == 4 ? 640 : 256; };
 
+// Pair p = i(i-1)/2 + j (i > j) of the flat lower triangle; the order does not depend on K, so one table serves
+// every K up to kQuadPairMaxK. Step s of a quad covers pairs 4 s .. 4 s + 3: their rows in the bytes of .x, their
+// columns in the bytes of .y (lane g takes byte g).
+constexpr int kQuadPairMaxK = 32;
+constexpr int kQuadPairSteps = (kQuadPairMaxK * (kQuadPairMaxK + 1) / 2 + kQuad - 1) / kQuad;
+struct QuadPairTable {
+  uint2 step[kQuadPairSteps];
+  constexpr QuadPairTable() : step() {
+    int i = 1, j = 0;
+    for (int s = 0; s < kQuadPairSteps; ++s) {
+      unsigned x = 0, y = 0;
+      for (int g = 0; g < kQuad; ++g) {
+        x |= (unsigned)i << (8 * g);
+        y |= (unsigned)j << (8 * g);
+        if (++j == i) {
+          j = 0;
+          ++i;
+        }
+      }
+      step[s] = uint2{x, y};
+    }
+  }
+};
+static __constant__ QuadPairTable kQuadPairs = QuadPairTable();
+
+template <typename T, int D> __device__ __forceinline__ void quad_load_slot(const T* __restrict__ src, T (&x)[D]) {
+  if constexpr (D == 3 && sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(src);
+    x[0] = v.x; x[1] = v.y; x[2] = v.z;
+  } else if constexpr (D == 2 && sizeof(T) == 4) {
+    const float2 v = *reinterpret_cast<const float2*>(src);
+    x[0] = v.x; x[1] = v.y;
+  } else if constexpr (D == 2 && sizeof(T) == 8) {
+    const double2 v = *reinterpret_cast<const double2*>(src);
+    x[0] = v.x; x[1] = v.y;
+  } else {
+#pragma unroll
+    for (int c = 0; c < D; ++c) x[c] = src[c];
+  }
+}
+
+constexpr int kQuadPairUnroll = 2;  // steps of the pair loop in flight together
+
 // Pair covariances of a point into tri[p] (p = i(i-1)/2 + j), dealt p = g, g+4, ... over the quad; pairs with
-// a padding slot (PAD, index >= kk) are 0.
+// a padding slot (PAD, index >= kk) are 0. Each step reads its (i, j) bytes from the warp-uniform constant table
+// and the lane picks its own with a byte permute; steps are independent, so an unrolled pair of them overlaps
+// its lookups. The point slots in crd are 16-byte aligned.
 template <typename T, int K, int D, bool PAD>
 __device__ __forceinline__ void quad_pairs(const T* __restrict__ crd, T* __restrict__ tri, int g, int kk,
                                            const TableView<T>& tab) {
   using SM = QuadSmem<K, D>;
-  int i = 1, j = g;
-  while (j >= i) { j -= i; ++i; }
-  for (int pp = g; pp < SM::kPairs; pp += kQuad) {
-    if (!GGP_CHECK(i <= K && j >= 0 && j < i, 302, i, j)) break;
+  static_assert(K <= kQuadPairMaxK, "pair table too small");
+  constexpr int kSteps = (SM::kPairs + kQuad - 1) / kQuad;
+  const unsigned sel = 0x4440u | (unsigned)g;  // byte g of the first operand, zeros above
+#pragma unroll kQuadPairUnroll
+  for (int st = 0; st < kSteps; ++st) {
+    if (SM::kPairs % kQuad != 0 && kQuad * st + g >= SM::kPairs) continue;
+    const uint2 ij = kQuadPairs.step[st];
+    const int i = (int)__byte_perm(ij.x, 0u, sel), j = (int)__byte_perm(ij.y, 0u, sel);
     T a = T(0);
     if (!(PAD && ((i < K && i >= kk) || j >= kk))) {
       T pi[D], pj[D];
-#pragma unroll
-      for (int c = 0; c < D; ++c) {
-        pi[c] = crd[i * SM::kPointStride + c];
-        pj[c] = crd[j * SM::kPointStride + c];
-      }
+      quad_load_slot<T, D>(crd + i * SM::kPointStride, pi);
+      quad_load_slot<T, D>(crd + j * SM::kPointStride, pj);
       a = tab(point_distance<T, D>(pi, pj));
     }
-    tri[pp] = a;
-    j += kQuad;
-    while (j >= i && i <= K) { j -= i; ++i; }
+    tri[kQuad * st + g] = a;
   }
 }
 
