@@ -221,16 +221,19 @@ static cudaError_t launch_knn_d(const PointSource<T, D>& src, long long n, int k
       // the heap kernels refill lanes from a global query counter: one resident wave of blocks
       const int max_blocks = (int)std::min<long long>((nq + 127) / 128, 1ll << 30);
       cudaMemsetAsync(next_query, 0, sizeof(unsigned long long), s);
+      const int levels = tree_levels(n);
       if (k <= 16) {
-        constexpr size_t smem = 16 * 128 * KnnHeapSmem<T>::bytes_per_entry;
+        const size_t smem = KnnHeapSmem<T>::bytes(16, 128, levels);
         auto kern = knn_heap_kernel<T, D, 16, int>;
         allow_smem(kern, smem);
-        (ggp::count_launch(), kern<<<persistent_grid(kern, 128, smem, max_blocks), 128, smem, s>>>(src, n, k, q, m, nq, q0, out, next_query));
+        (ggp::count_launch(), kern<<<persistent_grid(kern, 128, smem, max_blocks), 128, smem, s>>>(
+             src, n, k, q, m, nq, q0, out, next_query, levels));
       } else {
-        constexpr size_t smem = 32 * 128 * KnnHeapSmem<T>::bytes_per_entry;
+        const size_t smem = KnnHeapSmem<T>::bytes(32, 128, levels);
         auto kern = knn_heap_kernel<T, D, 32, int>;
         allow_smem(kern, smem);
-        (ggp::count_launch(), kern<<<persistent_grid(kern, 128, smem, max_blocks), 128, smem, s>>>(src, n, k, q, m, nq, q0, out, next_query));
+        (ggp::count_launch(), kern<<<persistent_grid(kern, 128, smem, max_blocks), 128, smem, s>>>(
+             src, n, k, q, m, nq, q0, out, next_query, levels));
       }
     }
   } else {
@@ -272,7 +275,12 @@ static int depths_device(const int* nbrs, long long n, long long n0, int k, int*
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, depths_kernel, 256, 0);
     if (per_sm < 1) per_sm = 1;
-    (ggp::count_launch(), depths_kernel<<<sms * per_sm, 256, 0, s>>>(nbrs, n, n0, k, depth, st, 10000000000ull));
+    // about 16 chunks of 32 rows per warp: the dependency chain, not the width, bounds a small graph, and a grid
+    // no wider than that leaves the other SMs to concurrent requests; a large graph gets every resident block
+    const long long chunks = (n - n0 + 31) / 32;
+    const long long want = (chunks + 16 * 8 - 1) / (16 * 8);
+    const int grid = (int)std::max<long long>(2, std::min<long long>((long long)sms * per_sm, want));
+    (ggp::count_launch(), depths_kernel<<<grid, 256, 0, s>>>(nbrs, n, n0, k, depth, st, 10000000000ull));
   }
   return g_status(cudaGetLastError());
 }

@@ -26,16 +26,41 @@ int list_warps_d(int d, int nb) {
   return d == 2 ? list_warps<K, 2>(nb) : list_warps<K, 3>(nb);
 }
 
-}  // namespace
-
-bool list_supported(int k, int d, int nb) {
+bool quad_list_supported(int k, int d, int nb) {
   if (k < 1 || k > kListMaxK || (d != 2 && d != 3)) return false;
   const int K = list_k(k);
   const int w = K == 8 ? list_warps_d<8>(d, nb) : (K == 16 ? list_warps_d<16>(d, nb) : list_warps_d<20>(d, nb));
   return w >= 1;
 }
 
+size_t list_warp_smem(int k, int d, bool logdet) {
+  return sizeof(double) * (size_t)list_warp_doubles(k, d, logdet) * (kListWarpBlock / 32);
+}
+
+bool list_warp_supported(int k, int d) {
+  if (k < 1 || k > kListWarpMaxK || d < 1) return false;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return list_warp_smem(k, d, false) + kSmemHeadroom <= (size_t)optin;
+}
+
+cudaError_t launch_list_warp(const RefineParams<float>& p, bool logdet, cudaStream_t s) {
+  const size_t smem = list_warp_smem(p.k, p.d, logdet);
+  auto kern = logdet ? refine_list_warp_kernel<true> : refine_list_warp_kernel<false>;
+  cudaError_t e = allow_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const int grid = persistent_grid(kern, kListWarpBlock, smem, logdet ? kMaxPartials : 0);
+  (ggp::count_launch(), kern<<<grid, kListWarpBlock, smem, s>>>(p));
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+bool list_supported(int k, int d, int nb) { return quad_list_supported(k, d, nb) || list_warp_supported(k, d); }
+
 cudaError_t launch_list(const RefineParams<float>& p, bool logdet, int nb, cudaStream_t s) {
+  if (!quad_list_supported(p.k, p.d, nb)) return launch_list_warp(p, logdet, s);
   const int K = list_k(p.k);
   if (p.d == 2) {
     if (K == 8) return launch_list_kd<8, 2>(p, logdet, nb, s);

@@ -205,9 +205,31 @@ __global__ void __launch_bounds__(128) knn_kernel(PointSource<T, D> src, long lo
 // into that slot and sifts it down (log k steps instead of rewriting and rescanning every slot), and the
 // final set is the same. Entry e of thread t lives at [e * blockDim + t]: conflict-free banks whatever entry
 // each thread touches.
+//
+// The walk keeps a stack instead of climbing back through the parents: every step visits a node. Descending
+// into the near child of a node at level l pushes the far child as "level l pending" with its squared split
+// distance (per-level slot in shared memory, plus a bitmask of pending levels); when a node has no child to
+// descend into, the deepest pending level whose split distance still satisfies sd^2 <= radius^2 (the radius
+// as it is now) gives the next node, and pending levels that fail are dropped. That is the decision the
+// reference's walk takes when it climbs back to that node from its near child, with the same radius, so both
+// visit the same nodes in the same order and keep the same slots; the climbing steps and their reloads of the
+// parents' records are gone. The far child needs no storage: in level order, node o of level l has children
+// o and o + 2^l of level l + 1, so the node of level L + 1 on the current path is the current node's offset
+// mod 2^(L+1), and the far child is that offset with bit L flipped.
 template <typename T> struct KnnHeapSmem {
   static constexpr size_t bytes_per_entry = sizeof(T) + sizeof(int) + 1;
+  // shared memory of one block: the heaps, and one squared split distance per tree level and thread
+  static size_t bytes(int kmax, int block, int levels) {
+    return (size_t)block * (kmax * bytes_per_entry + (size_t)levels * sizeof(T));
+  }
 };
+
+// Tree levels holding the indices 0 .. n-1 (level l holds 2^l - 1 .. 2^(l+1) - 2).
+inline int tree_levels(long long n) {
+  int l = 0;
+  while (l < 62 && ((2ll << l) - 1) < n) ++l;
+  return l + 1;
+}
 
 // Lanes are refilled: once no more than kKnnRefillAt lanes of a warp are still traversing (the stragglers),
 // every idle lane writes its finished result and takes a new query. The idle lanes take consecutive queries from
@@ -225,14 +247,15 @@ __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, lo
                                                        const int* __restrict__ query_idx,
                                                        const int* __restrict__ max_idx, long long nq, long long q0,
                                                        int* __restrict__ out,
-                                                       unsigned long long* __restrict__ next_query) {
+                                                       unsigned long long* __restrict__ next_query, int levels) {
   constexpr int PD = D > 0 ? D : kKnnMaxD;
   constexpr unsigned kFull = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char knn_smem[];
   const int bd = blockDim.x;
   T* hd = reinterpret_cast<T*>(knn_smem) + threadIdx.x;
   int* hi = reinterpret_cast<int*>(knn_smem + sizeof(T) * KMAX * bd) + threadIdx.x;
-  unsigned char* hs = knn_smem + (sizeof(T) + sizeof(int)) * KMAX * bd + threadIdx.x;
+  T* sdl = reinterpret_cast<T*>(knn_smem + (sizeof(T) + sizeof(int)) * KMAX * bd) + threadIdx.x;  // per level
+  unsigned char* hs = knn_smem + (sizeof(T) + sizeof(int)) * KMAX * bd + sizeof(T) * levels * bd + threadIdx.x;
   const T inf = (T)INFINITY;
   const unsigned lanes_below = (1u << (threadIdx.x & 31)) - 1u;
   bool more = true;      // warp-uniform: the counter has not yet passed nq
@@ -241,7 +264,8 @@ __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, lo
   bool fin = false;      // traversal ended, result not yet written
   T q[PD];
   T maxv = inf;
-  IDX mxi = 0, cur = -1, prev = -1;
+  IDX mxi = 0, cur = -1;
+  unsigned int pend = 0;  // levels with a far child still to consider
   for (;;) {
     const unsigned live_mask = __ballot_sync(kFull, live);
     if (__popc(live_mask) <= kKnnRefillAt) {
@@ -312,58 +336,72 @@ __global__ void __launch_bounds__(128) knn_heap_kernel(PointSource<T, D> src, lo
           maxv = inf;
           mxi = (IDX)mx;
           cur = 0;  // the root is visited whatever the limit (tree.py _traverse_tree starts there)
-          prev = -1;
+          pend = 0;
           live = true;
         }
       }
       if (__ballot_sync(kFull, live || fin) == 0) break;
     }
     for (int r = 0; r < kKnnStepsPerCheck && live; ++r) {
-      const IDX par = tree_parent(cur);
       T p[PD];
       int s;
       src.load(cur, p, s);
-      if (prev == par) {
-        const T d2 = sqdist<T, D>(q, p, src.d);
-        if (d2 < maxv) {
-          const int ns = hs[0];
-          int i = 0;
-          for (;;) {
-            const int l = 2 * i + 1;
-            if (l >= k) break;
-            int c = l;
-            T cd = hd[l * bd];
-            int cs = hs[l * bd];
-            if (l + 1 < k) {
-              const T rd = hd[(l + 1) * bd];
-              const int rs = hs[(l + 1) * bd];
-              if (rd > cd || (rd == cd && rs < cs)) { c = l + 1; cd = rd; cs = rs; }
-            }
-            if (cd > d2 || (cd == d2 && cs < ns)) {
-              hd[i * bd] = cd;
-              hs[i * bd] = (unsigned char)cs;
-              hi[i * bd] = hi[c * bd];
-              i = c;
-            } else {
-              break;
-            }
+      const T d2 = sqdist<T, D>(q, p, src.d);
+      if (d2 < maxv) {
+        const int ns = hs[0];
+        int i = 0;
+        for (;;) {
+          const int l = 2 * i + 1;
+          if (l >= k) break;
+          int c = l;
+          T cd = hd[l * bd];
+          int cs = hs[l * bd];
+          if (l + 1 < k) {
+            const T rd = hd[(l + 1) * bd];
+            const int rs = hs[(l + 1) * bd];
+            if (rd > cd || (rd == cd && rs < cs)) { c = l + 1; cd = rd; cs = rs; }
           }
-          hd[i * bd] = d2;
-          hs[i * bd] = (unsigned char)ns;
-          hi[i * bd] = (int)cur;
-          maxv = hd[0];
+          if (cd > d2 || (cd == d2 && cs < ns)) {
+            hd[i * bd] = cd;
+            hs[i * bd] = (unsigned char)cs;
+            hi[i * bd] = hi[c * bd];
+            i = c;
+          } else {
+            break;
+          }
         }
+        hd[i * bd] = d2;
+        hs[i * bd] = (unsigned char)ns;
+        hi[i * bd] = (int)cur;
+        maxv = hd[0];
       }
       const T sd = rn_sub(coord<T, D>(q, s), coord<T, D>(p, s));
+      const T sd2 = rn_mul(sd, sd);
       const int lvl = tree_level((IDX)(cur + 1));
       const IDX left = cur + ((IDX)1 << lvl), right = cur + ((IDX)2 << lvl);
       const IDX nearc = sd < T(0) ? left : right;
       const IDX farc = sd < T(0) ? right : left;
-      const bool far_in = rn_mul(sd, sd) <= maxv;
-      IDX next;
-      if (prev == nearc || (prev == par && nearc >= mxi)) next = (farc < mxi && far_in) ? farc : par;
-      else next = (prev == par) ? nearc : par;
-      prev = cur;
+      IDX next = -1;
+      if (nearc < mxi) {
+        if (farc < mxi) {
+          sdl[lvl * bd] = sd2;
+          pend |= 1u << lvl;
+        }
+        next = nearc;
+      } else if (farc < mxi && sd2 <= maxv) {
+        next = farc;
+      } else {
+        const IDX off = cur - (((IDX)1 << lvl) - 1);  // offset of cur in its level
+        while (pend) {
+          const int L = 31 - __clz(pend);
+          pend &= ~(1u << L);
+          if (sdl[L * bd] <= maxv) {
+            const IDX m = ((IDX)2 << L) - 1;  // first index of level L + 1, and the offset mask
+            next = m + ((off & m) ^ ((IDX)1 << L));
+            break;
+          }
+        }
+      }
       cur = next;
       if (cur == -1) {
         live = false;

@@ -44,17 +44,12 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
   }
   const size_t smem = table_smem_bytes<T>(nb);
   if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, 4);
-  if (kind == kCond) {
-    auto kern = refine_quad_kernel<T, K, D, PAD, false>;
-    allow_smem(kern, smem);
-    const int grid = persistent_grid(kern, 128, smem, max_blocks);
-    (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));
-  } else {
-    auto kern = refine_quad_kernel<T, K, D, PAD, true>;
-    allow_smem(kern, smem);
-    const int grid = persistent_grid(kern, 128, smem, max_blocks);
-    (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));
-  }
+  auto kern = (kind != kCond) ? refine_quad_kernel<T, K, D, PAD, kOpLogdet>
+              : (p.mode == kGenerate ? refine_quad_kernel<T, K, D, PAD, kOpGenerate>
+                                     : refine_quad_kernel<T, K, D, PAD, kOpInverse>);
+  allow_smem(kern, smem);
+  const int grid = persistent_grid(kern, 128, smem, max_blocks);
+  (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));
   return cudaGetLastError();
 }
 

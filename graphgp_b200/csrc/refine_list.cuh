@@ -118,6 +118,127 @@ __global__ void __launch_bounds__(256) refine_list_kernel(RefineParams<float> p)
   }
 }
 
+// The same second pass for shapes outside the quad instantiations (k > kListMaxK, or d not in {2, 3}): one warp
+// per listed point, its packed joint matrix in shared memory (rows 0..k-1 neighbours, k the point itself and, for
+// the inverse, a last row holding the neighbour values, so that the right-looking Cholesky leaves L11^-1 v there:
+// mean = L[k, :k] . (L11^-1 v), std = L[k, k]), FP64 throughout, the FP64 table read through the cache.
+constexpr int kListWarpMaxK = 64;
+constexpr int kListWarpBlock = 128;
+
+__device__ __forceinline__ int list_packed(int i, int j) { return i * (i + 1) / 2 + j; }
+
+// Doubles of shared memory per warp: the packed matrix, the coordinates, the neighbour ids (two per double),
+// rounded up to an even count (16-byte aligned warps).
+__host__ __device__ inline int list_warp_doubles(int k, int d, bool logdet) {
+  const int nr = logdet ? k + 1 : k + 2;
+  const int n = nr * (nr + 1) / 2 + (k + 1) * d + (k + 1) / 2;
+  return (n + 1) / 2 * 2;
+}
+
+template <bool LOGDET>
+__global__ void __launch_bounds__(kListWarpBlock) refine_list_warp_kernel(RefineParams<float> p) {
+  extern __shared__ __align__(16) double lw_smem[];
+  __shared__ double s_part[kListWarpBlock / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k = p.k, d = p.d;
+  const int nr = LOGDET ? k + 1 : k + 2;
+  double* A = lw_smem + (size_t)warp * list_warp_doubles(k, d, LOGDET);
+  double* crd = A + nr * (nr + 1) / 2;
+  int* ids = reinterpret_cast<int*>(crd + (k + 1) * d);
+  const TableView<double> tab = global_table_view<double>(p.tb);
+  const double c0 = p.tb.desc->c0;
+  unsigned int count = (unsigned int)ld_relaxed(reinterpret_cast<const int*>(&p.status->listed));
+  if ((long long)count > p.n - p.n0) count = (unsigned int)(p.n - p.n0);
+  double acc_logdet = 0.0;
+  for (;;) {
+    const unsigned int t = warp_ticket(&p.status->ticket2);
+    if (t >= count) break;
+    long long row = (long long)__ldg(p.fb_rows + t);
+    if (!GGP_CHECK(row >= p.n0 && row < p.n, 204, row, t) || row < p.n0 || row >= p.n) row = p.n0;
+    const long long r0 = row - p.n0;
+    for (int m = lane; m < k; m += 32) {
+      int id = __ldg(p.nbrs + r0 * k + m);
+      ids[m] = (id < 0 || (long long)id >= p.n) ? 0 : id;  // the first pass reported it already
+    }
+    __syncwarp();
+    for (int e = lane; e < (k + 1) * d; e += 32) {
+      const int i = e / d, c = e - i * d;
+      const long long pid = i < k ? (long long)ids[i] : row;
+      crd[e] = (double)__ldg(p.points + pid * d + c);
+    }
+    if (!LOGDET) {
+      for (int m = lane; m < k; m += 32) A[list_packed(k + 1, m)] = (double)__ldg(p.values + ids[m]);
+      if (lane == 0) {
+        A[list_packed(k + 1, k)] = 0.0;
+        A[list_packed(k + 1, k + 1)] = 1.0;
+      }
+    }
+    __syncwarp();
+    for (int i = 0; i <= k; ++i) {
+      for (int j = lane; j <= i; j += 32) {
+        double v = c0;
+        if (j != i) {
+          double s2 = 0.0;
+          for (int c = 0; c < d; ++c) {
+            const double df = crd[i * d + c] - crd[j * d + c];
+            s2 = fma(df, df, s2);
+          }
+          v = tab(sqrt(s2));
+        }
+        A[list_packed(i, j)] = v;
+      }
+    }
+    __syncwarp();
+    // right-looking Cholesky over columns 0..k; the value row (inverse) is updated like the others
+    for (int j = 0; j <= k; ++j) {
+      const double djj = sqrt(A[list_packed(j, j)]);
+      for (int i = j + 1 + lane; i < nr; i += 32) A[list_packed(i, j)] /= djj;
+      __syncwarp();
+      if (lane == 0) A[list_packed(j, j)] = djj;
+      for (int i = j + 1; i < nr; ++i) {
+        const double lij = A[list_packed(i, j)];
+        const int mmax = i <= k ? i : k;
+        for (int m = j + 1 + lane; m <= mmax; m += 32) A[list_packed(i, m)] -= lij * A[list_packed(m, j)];
+      }
+      __syncwarp();
+    }
+    if (LOGDET) {
+      if (lane == 0) {
+        const double l = log(A[list_packed(k, k)]);
+        if (l != l) atomicOr(&p.status->nan_seen, 1u);
+        acc_logdet += l;
+      }
+    } else {
+      double mu = 0.0;
+      for (int m = lane; m < k; m += 32) mu = fma(A[list_packed(k, m)], A[list_packed(k + 1, m)], mu);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mu += __shfl_xor_sync(0xffffffffu, mu, o);
+      if (lane == 0) {
+        const float out = canonical((float)(((double)__ldg(p.values + row) - mu) / A[list_packed(k, k)]));
+        if (out != out) atomicOr(&p.status->nan_seen, 1u);
+        if (p.out_user) {
+          const int u = __ldg(p.perm + row);
+          if (GGP_CHECK(u >= 0 && u < p.n, 205, u, row)) p.out_user[u] = out;
+        } else {
+          p.xi_out[r0] = out;
+        }
+      }
+    }
+    __syncwarp();  // the scratch is reused by the next point
+  }
+  if (LOGDET) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc_logdet += __shfl_xor_sync(0xffffffffu, acc_logdet, o);
+    if (lane == 0) s_part[warp] = acc_logdet;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += s_part[w];
+      if (s != 0.0) atomicAdd(p.logdet_partials + (blockIdx.x % kMaxPartials), s);
+    }
+  }
+}
+
 // Warps per block of the list pass for a table of nb entries (0: the FP64 table leaves no room for one warp).
 template <int K, int D>
 inline int list_warps(int nb) {
@@ -133,7 +254,8 @@ inline int list_warps(int nb) {
 // Instantiated shapes: K = 8, 16, 20 (padded up from k), D = 2, 3 (inst/list.cu).
 inline int list_k(int k) { return k <= 8 ? 8 : (k <= 16 ? 16 : 20); }
 
-// True when the FP32 inverse / logdet of this shape can leave its ill-conditioned points to the list pass.
+// True when the FP32 inverse / logdet of this shape can leave its ill-conditioned points to a list pass (the quad
+// list kernel for k <= kListMaxK and d in {2, 3}, else the warp-per-point kernel for k <= kListWarpMaxK).
 bool list_supported(int k, int d, int nb);
 
 // The FP64 list pass after an FP32 inverse (logdet = false) or log-determinant pass on the same stream.

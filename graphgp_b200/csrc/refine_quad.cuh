@@ -293,9 +293,12 @@ __device__ __forceinline__ void quad_finish(const RefineParams<T>& p, bool gen, 
   }
 }
 
-// Generate (mode kGenerate) / inverse (kInverse) / log-determinant (LOGDET).
-template <typename T, int K, int D, bool PAD, bool LOGDET>
+// Generate / inverse / log-determinant (MODE: kOpGenerate, kOpInverse, kOpLogdet, fixed at compile time). With a
+// row list (RefineParams::fb_rows), the inverse and log-determinant leave their points below tau to the FP64
+// second pass instead of re-conditioning them here.
+template <typename T, int K, int D, bool PAD, int MODE>
 __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
+  constexpr bool LOGDET = MODE == kOpLogdet;
   constexpr int NT = QuadRows<K>::NT;
   extern __shared__ __align__(32) unsigned char smem[];
   __shared__ double s_part[4];
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
   const int g = lane & (kQuad - 1);
   const int q = lane >> 2;
   const int src0 = lane & ~(kQuad - 1);
-  const bool gen = !LOGDET && p.mode == kGenerate;
+  constexpr bool gen = MODE == kOpGenerate;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
@@ -331,16 +334,20 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
       quad_factor<T, K, D, PAD>(P, g, src0, p.k, tab, c0, wmine, var, mr);
       mr = quad_min(mr);
       const bool fb = sizeof(T) == 4 && active && !(mr >= (T)p.tau);  // quad-uniform
+      const bool defer = !gen && fb && p.fb_rows != nullptr;  // constant false in the generate instantiation
       double w64[K];
       double vd64 = 0.0;
-      if (fb && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
+      if (fb && !defer && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
       T mean = T(0);
       if (!LOGDET) mean = quad_mean<T, K>(p, gen, may_wait, ids, g, wmine, ok);
       // quad-wide AND; every lane executes both shuffles (no short-circuit around a warp intrinsic)
       int okv = ok ? 1 : 0;
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
-      if (active && g == 0) quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
+      if (active && g == 0) {
+        if (defer) list_row(p, row);
+        else quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
+      }
     }
   }
   if (LOGDET) {

@@ -205,3 +205,27 @@ def test_invalid_graph_reports_not_hangs(cuda_device):
     st = gc.last_status()
     assert st["error"] == 1
     assert torch.isnan(out[g.offsets[0]]).item()
+
+
+@pytest.mark.parametrize("k,d", [(32, 3), (24, 2)])
+def test_inverse_logdet_list_pass_k32(cuda_device, k, d):
+    """k above the quad list kernel's sizes: the FP32 first pass lists its points below tau and the
+    warp-per-point FP64 pass finishes them; inverse and logdet stay within the FP32 bar of the FP64 oracle."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    n, n0 = 2500, 128
+    pts, g = oracle_graph(n, d, n0, k, seed=11)
+    bins, vals = as_inputs(rbf_table(scale=0.5), np.float32)
+    f32 = torch.float32
+    args = (_t(g.points, cuda_device), _t(g.neighbors, cuda_device), g.offsets, _t(bins, cuda_device, f32),
+            _t(vals, cuda_device, f32))
+    v = np.random.default_rng(2).standard_normal(n).astype(np.float32)
+    i0, xi = gc.refine_inv(*args, _t(v, cuda_device, f32))
+    listed = int(gc._tls.last_ws[:64].view(torch.int32)[7].item())
+    assert listed > 0  # the smooth table puts points below the inverse threshold
+    ri0, rxi = orf.refine_inv(g.points, g.neighbors, g.offsets, (bins, vals), v)
+    assert rel_err(xi.cpu().numpy(), rxi) < TOL32
+    ld = float(gc.refine_logdet(*args))
+    rld = orf.refine_logdet(g.points, g.neighbors, g.offsets, (bins, vals))
+    assert abs(ld - rld) / abs(rld) < TOL32
