@@ -101,6 +101,11 @@ _SIGS = {
     "ggp_request_buffer_size": ([_I, _I64, _I, _I64, _I, _I, _I], _SZ),
     "ggp_request_f32": ([_I, _P, _I64, _I, _I64, _I, _P, _P, _I, _P, _P, _P, _D, _P, _SZ, _P], _I),
     "ggp_request_f64": ([_I, _P, _I64, _I, _I64, _I, _P, _P, _I, _P, _P, _P, _P, _SZ, _P], _I),
+    "ggp_request_host_sizes": ([_I, _I64, _I, _I64, _I, _I, _I, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)], _I),
+    "ggp_request_host_f32": ([_I, _P, _I64, _I, _I64, _I, _P, _P, _I, _P, _P, _P, C.POINTER(Status), _D, _P, _SZ,
+                              _P, _SZ, _P], _I),
+    "ggp_request_host_f64": ([_I, _P, _I64, _I, _I64, _I, _P, _P, _I, _P, _P, _P, C.POINTER(Status), _P, _SZ, _P,
+                              _SZ, _P], _I),
 }
 
 _lib = None

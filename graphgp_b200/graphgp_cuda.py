@@ -15,6 +15,8 @@ from __future__ import annotations
 import ctypes as C
 import threading
 
+import numpy as np
+
 import torch
 
 from . import _lib
@@ -462,6 +464,65 @@ def request(op, points, n0, k, cov_bins, cov_vals, payload=None, *, tau=None):
                                  _stream())
     _lib.check(rc, "request")
     return out if m < 2 else ld
+
+
+def request_host(op, points, n0, k, cov_bins, cov_vals, payload=None, *, tau=None, buffers=None, device=None):
+    """``request`` with host (numpy) arrays end to end (``ggp_request_host_*``): the inputs go up through a pinned
+    staging block in one copy, the graph build and operation run on the current stream, and the result and the
+    status block come back before the call returns, all inside one native call. Returns (output, status dict):
+    output is the (N,) numpy array in the caller's order, or the float log-determinant. ``buffers`` (a dict)
+    keeps the device and pinned blocks between calls, grown when a request needs more."""
+    if op not in _REQUEST_OPS:
+        raise ValueError(f"unknown op {op!r}")
+    if n0 < k:
+        raise ValueError(f"n0 must be at least k. Got n0={n0}, k={k}.")
+    pts = np.asarray(points)
+    if pts.ndim != 2:
+        raise ValueError(f"Points must have shape (N, d). Got shape {tuple(pts.shape)}.")
+    dt = np.float64 if pts.dtype == np.float64 else np.float32
+    pts = np.ascontiguousarray(pts, dt)
+    n, d = pts.shape
+    if n0 > n:
+        raise ValueError("n0 must not exceed the number of points")
+    bins = np.ascontiguousarray(cov_bins, dt)
+    vals = np.ascontiguousarray(cov_vals, dt)
+    if bins.ndim != 1 or vals.shape != bins.shape or len(bins) < 2:
+        raise ValueError("cov_bins and cov_vals must be 1-D arrays of equal length >= 2")
+    m = _REQUEST_OPS[op]
+    x = None
+    out = None
+    if m < 2:
+        x = np.ascontiguousarray(payload, dt).reshape(-1)
+        if x.size != n:
+            raise ValueError("payload must have one entry per point")
+        out = np.empty(n, dt)
+    lib = _lib.load()
+    dev_b, pin_b = C.c_size_t(), C.c_size_t()
+    _lib.check(lib.ggp_request_host_sizes(m, n, d, int(n0), int(k), len(bins), np.dtype(dt).itemsize,
+                                          C.byref(dev_b), C.byref(pin_b)), "request_host")
+    buffers = {} if buffers is None else buffers
+    device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    dbuf = buffers.get("device")
+    if dbuf is None or dbuf.numel() < dev_b.value or dbuf.device != device:
+        dbuf = buffers["device"] = torch.empty(max(dev_b.value, 1 << 20), dtype=torch.uint8, device=device)
+    pbuf = buffers.get("pinned")
+    if pbuf is None or pbuf.numel() < pin_b.value:
+        pbuf = buffers["pinned"] = torch.empty(max(pin_b.value, 1 << 20), dtype=torch.uint8, pin_memory=True)
+    _tls.last_ws = dbuf
+    ld = C.c_double(0.0)
+    st = _lib.Status()
+    addr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+    if dt == np.float32:
+        rc = lib.ggp_request_host_f32(m, addr(pts), n, d, int(n0), int(k), addr(bins), addr(vals), len(bins), addr(x),
+                                      addr(out), C.byref(ld), C.byref(st), _tau(tau), dbuf.data_ptr(), dbuf.numel(),
+                                      pbuf.data_ptr(), pbuf.numel(), _stream())
+    else:
+        rc = lib.ggp_request_host_f64(m, addr(pts), n, d, int(n0), int(k), addr(bins), addr(vals), len(bins), addr(x),
+                                      addr(out), C.byref(ld), C.byref(st), dbuf.data_ptr(), dbuf.numel(),
+                                      pbuf.data_ptr(), pbuf.numel(), _stream())
+    _lib.check(rc, "request_host")
+    status = dict(error=st.error, nan_seen=st.nan_seen, fallback_count=st.fallback_count, timeouts=st.timeouts)
+    return (out if m < 2 else float(ld.value)), status
 
 
 def wait_probe(timeout_ns=1_000_000):

@@ -184,6 +184,40 @@ class Scheduler:
         return results, now()
 
 
+class _Slot:
+    """A worker's device state: its CUDA stream and pinned host staging buffers. Uploads go numpy -> pinned
+    buffer (a host memcpy) -> device on the slot's stream, and results come back into a pinned buffer; copies
+    from or to pageable memory would all pass through the driver's one staging path and serialise the slots. A
+    slot runs one request at a time and waits for its result before the next one reuses the buffers."""
+
+    def __init__(self, torch, device, stream=None):
+        self.torch = torch
+        self.stream = stream if stream is not None else torch.cuda.Stream(device=device)
+        self._bufs = {}
+        self.native = {}  # device and pinned blocks of the one-call host path (graphgp_cuda.request_host)
+
+    def pinned(self, name, numel, dtype):
+        t = self._bufs.get(name)
+        if t is None or t.numel() < numel or t.dtype != dtype:
+            t = self.torch.empty(max(int(numel), 1024), dtype=dtype, pin_memory=True)
+            self._bufs[name] = t
+        return t[:numel]
+
+    def upload(self, name, array, dtype, device):
+        """A numpy array -> a device tensor of the same shape, through this slot's pinned buffer."""
+        a = np.ascontiguousarray(array)
+        host = self.pinned(name, a.size, dtype).view(a.shape)
+        host.copy_(self.torch.from_numpy(a))
+        return host.to(device, non_blocking=True)
+
+    def download(self, name, tensor):
+        """A device tensor -> numpy (a copy), through this slot's pinned buffer; waits on the slot's stream."""
+        host = self.pinned(f"{name}_{tensor.dtype}", tensor.numel(), tensor.dtype).view(tensor.shape)
+        host.copy_(tensor, non_blocking=True)
+        self.stream.synchronize()
+        return host.numpy().copy()
+
+
 class Engine:
     """The device side: each slot owns a CUDA stream; a request uploads its inputs, builds its graph, runs its
     operation and reads its result back on that stream. Graphs (``Request.graph_key``) and kernel tables
@@ -216,7 +250,7 @@ class Engine:
     def _slot_init(self):
         torch = self.torch
         torch.cuda.set_device(self.device)
-        return torch.cuda.Stream(device=self.device)
+        return _Slot(torch, self.device)
 
     def _cached(self, cache, key, make):
         if key is None:
@@ -229,40 +263,42 @@ class Engine:
                 v = cache.setdefault(key, v)
         return v
 
-    def process(self, req: Request, stream=None):
-        """One request on ``stream`` (default: the current stream); returns (output, status dict)."""
+    def process(self, req: Request, slot=None):
+        """One request on ``slot`` (a worker's slot, a CUDA stream, or None for the current stream); returns
+        (output, status dict)."""
         torch, gc, dev = self.torch, self.gc, self.device
-        stream = stream or torch.cuda.current_stream(dev)
-        with torch.cuda.stream(stream), torch.cuda.nvtx.range(f"request {req.rid} {req.op} n={req.n}"):
+        if not isinstance(slot, _Slot):
+            slot = _Slot(torch, dev, stream=slot or torch.cuda.current_stream(dev))
+        dt = self.dtype
+        with torch.cuda.stream(slot.stream), torch.cuda.nvtx.range(f"request {req.rid} {req.op} n={req.n}"):
 
             def make_graph():
-                P = torch.from_numpy(np.ascontiguousarray(req.points, self._np)).to(dev, non_blocking=True)
+                P = slot.upload("points", req.points, dt, dev)
                 return gc.build_graph(P, n0=req.n0, k=req.k, return_offsets=True)
 
             def make_table():
-                return (torch.as_tensor(np.asarray(req.bins), dtype=self.dtype).to(dev, non_blocking=True),
-                        torch.as_tensor(np.asarray(req.vals), dtype=self.dtype).to(dev, non_blocking=True))
+                return slot.upload("bins", req.bins, dt, dev), slot.upload("vals", req.vals, dt, dev)
 
+            if req.op not in OPS:
+                raise ValueError(f"unknown op {req.op!r}")
             if self.fused and req.graph_key is None and req.table_key is None:
-                # nothing resident to reuse: graph build and operation in one native call
-                P = torch.from_numpy(np.ascontiguousarray(req.points, self._np)).to(dev, non_blocking=True)
-                B, V = make_table()
-                x = None
-                if req.op in ("generate", "inverse"):
-                    x = torch.from_numpy(np.ascontiguousarray(req.payload, self._np)).to(dev, non_blocking=True)
-                r = gc.request(req.op, P, req.n0, req.k, B, V, x, tau=self.tau)
-                out = float(r.item()) if req.op == "logdet" else r.cpu().numpy()
-                return out, gc.last_status()
+                # nothing resident to reuse: staging, upload, graph build, operation, readback and status in one
+                # native call that holds no Python lock
+                return gc.request_host(req.op, np.asarray(req.points, self._np), req.n0, req.k, req.bins, req.vals,
+                                       req.payload if req.op != "logdet" else None, tau=self.tau, buffers=slot.native,
+                                       device=dev)
+            # a resident graph and / or table: separate calls on the device tensors
+            x = slot.upload("payload", req.payload, dt, dev) if req.op != "logdet" else None
             gp, gi, gn, _, offs = self._cached(self._graphs, req.graph_key, make_graph)
             B, V = self._cached(self._tables, req.table_key, make_table)
-            if req.op in ("generate", "inverse"):
-                x = torch.from_numpy(np.ascontiguousarray(req.payload, self._np)).to(dev, non_blocking=True)
-                f = gc.generate if req.op == "generate" else gc.generate_inv
-                out = f(gp, gi, gn, offs, B, V, x, tau=self.tau).cpu().numpy()
-            elif req.op == "logdet":
-                out = float(gc.generate_logdet(gp, gn, offs, B, V, tau=self.tau).item())
+            if req.op == "generate":
+                r = gc.generate(gp, gi, gn, offs, B, V, x, tau=self.tau)
+            elif req.op == "inverse":
+                r = gc.generate_inv(gp, gi, gn, offs, B, V, x, tau=self.tau)
             else:
-                raise ValueError(f"unknown op {req.op!r}")
+                r = gc.generate_logdet(gp, gn, offs, B, V, tau=self.tau)
+            out = slot.download("out", r.reshape(-1))
+            out = float(out[0]) if req.op == "logdet" else out
             return out, gc.last_status()
 
     def footprint(self, req: Request) -> int:

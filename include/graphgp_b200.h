@@ -295,6 +295,24 @@ int ggp_request_f64(int op, const double* points, int64_t n, int d, int64_t n0, 
                     const double* cov_vals, int n_bins, const double* payload, double* out_values,
                     double* out_logdet, void* buffer, size_t buffer_bytes, ggp_stream_t stream);
 
+/* The same request with every array on the HOST: `points`, `cov_bins`, `cov_vals`, `payload` are read  */
+/* and `out_values` / `*out_logdet` / `*out_status` written in host memory. The inputs are packed into */
+/* `pinned` (page-locked host memory, ggp_request_host_sizes bytes), copied to the device in one      */
+/* transfer on `stream`, the request runs as above in `buffer` (device, 256-byte aligned), and the    */
+/* result and the status block come back through `pinned`. The call returns when the result is in   */
+/* host memory; a caller that drives several streams from several threads calls it without holding   */
+/* any lock of its own. `out_status` may be null. Returns GGP_ERR_WORKSPACE when a buffer is short.   */
+int ggp_request_host_sizes(int op, int64_t n, int d, int64_t n0, int k, int n_bins, int dtype_bytes,
+                           size_t* device_bytes, size_t* pinned_bytes);
+int ggp_request_host_f32(int op, const float* points, int64_t n, int d, int64_t n0, int k, const float* cov_bins,
+                         const float* cov_vals, int n_bins, const float* payload, float* out_values,
+                         double* out_logdet, ggp_status_t* out_status, double tau, void* buffer,
+                         size_t buffer_bytes, void* pinned, size_t pinned_bytes, ggp_stream_t stream);
+int ggp_request_host_f64(int op, const double* points, int64_t n, int d, int64_t n0, int k,
+                         const double* cov_bins, const double* cov_vals, int n_bins, const double* payload,
+                         double* out_values, double* out_logdet, ggp_status_t* out_status, void* buffer,
+                         size_t buffer_bytes, void* pinned, size_t pinned_bytes, ggp_stream_t stream);
+
 /* ---------------------------------------------------------------------------------------------- */
 /* Failure-detection probe: launches one kernel whose single wait watches a flag that nothing sets,  */
 /* bounded by timeout_ns; returns GGP_ERR_TIMEOUT in *out_code (host int) when the bound worked.      */

@@ -161,3 +161,29 @@ def test_concurrent_requests_with_different_table_sizes(cuda_device):
         out, st = alone.process(r)
         assert m.status["error"] == 0 and st["error"] == 0
         assert _same(m.output, out, r.op), (r.rid, len(r.bins))
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_request_host_equals_device_request(cuda_device, dtype):
+    """The one-call host path (ggp_request_host_*: pinned staging, upload, build, operation, readback, status)
+    gives what the device-tensor request gives on the same inputs (bit-identical values; the log-determinant's
+    FP64 partial sums within 1e-12)."""
+    import torch
+
+    from graphgp_b200 import graphgp_cuda as gc
+
+    tdt = getattr(torch, dtype)
+    buffers = {}
+    for r in _stream(6, seed=5):
+        pts = np.asarray(r.points, dtype)
+        P = torch.as_tensor(pts, device=cuda_device)
+        B = torch.as_tensor(np.asarray(r.bins), dtype=tdt, device=cuda_device)
+        V = torch.as_tensor(np.asarray(r.vals), dtype=tdt, device=cuda_device)
+        pay = None if r.op == "logdet" else np.asarray(r.payload, dtype)
+        dev_out = gc.request(r.op, P, r.n0, r.k, B, V, None if pay is None else torch.as_tensor(pay, device=cuda_device))
+        ref = float(dev_out.item()) if r.op == "logdet" else dev_out.cpu().numpy()
+        out, st = gc.request_host(r.op, pts, r.n0, r.k, r.bins, r.vals, pay, buffers=buffers, device=cuda_device)
+        assert st["error"] == 0
+        if r.op != "logdet":
+            assert out.dtype == np.dtype(dtype)
+        assert _same(out, ref, r.op)
