@@ -404,4 +404,128 @@ cudaError_t launch_dense_root(const DenseRootArgs<T>& args, cudaStream_t s) {
                                      s);
 }
 
+// ------------------------------------------------------------------------------------------------
+// M <- M L^-1 in place (solve X L = M), L lower triangular n x n and M n x n, both row-major: the dense-root
+// adjoint's two triangular solves. One cooperative launch, 64 x 64 tiles, tile columns J from last to first:
+//   A. block t takes tile row I = t: X_IJ = M_IJ L_JJ^-1 by backward substitution over the 64 columns of the
+//      diagonal tile, four threads per matrix row with 16 columns each in registers (no block barrier inside);
+//   B. grid barrier; every block takes tiles (I, K), K < J: M_IK -= X_IJ L_JK; grid barrier.
+// ------------------------------------------------------------------------------------------------
+struct DenseTrsmSmem {
+  double A[kDenseTile][kDenseLd];  // phase A: L_JJ (row-major); phase B: X_IJ, k-major
+  double B[kDenseTile][kDenseLd];  // phase B: L_JK (row-major)
+  double rdiag[kDenseTile];
+};
+
+// Phase A for tile row I and tile column J.
+__device__ __forceinline__ void dense_trsm_diag(double* __restrict__ M, const double* __restrict__ L, long long n,
+                                                int I, int J, DenseTrsmSmem& s) {
+  const long long oj = (long long)J * kDenseTile;
+  const int nb = (int)((n - oj) < kDenseTile ? (n - oj) : kDenseTile);
+  __syncthreads();  // the previous use of the shared tiles is over
+  for (int e = threadIdx.x; e < kDenseTile * kDenseTile; e += kDenseThreads) {
+    const int r = e >> 6, c = e & 63;
+    s.A[r][c] = (r < nb && c < nb) ? (c <= r ? L[(oj + r) * n + oj + c] : 0.0) : (r == c ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  if (threadIdx.x < kDenseTile) s.rdiag[threadIdx.x] = 1.0 / s.A[threadIdx.x][threadIdx.x];
+  __syncthreads();
+  const int pr = threadIdx.x >> 2, q = threadIdx.x & 3;
+  const long long row = (long long)I * kDenseTile + pr;
+  const bool valid = row < n;
+  double* mrow = M + (valid ? row : 0) * n + oj;
+  double x[kDenseTile / 4];  // columns 4 s + q of this row
+#pragma unroll
+  for (int k = 0; k < kDenseTile / 4; ++k) {
+    const int c = 4 * k + q;
+    x[k] = (valid && c < nb) ? mrow[c] : 0.0;
+  }
+#pragma unroll
+  for (int c = kDenseTile - 1; c >= 0; --c) {
+    const double own = x[c >> 2] * s.rdiag[c];
+    const double xc = __shfl_sync(0xffffffffu, own, (threadIdx.x & 31 & ~3) | (c & 3));
+    if (q == (c & 3)) x[c >> 2] = xc;
+#pragma unroll
+    for (int k = 0; k < kDenseTile / 4; ++k)
+      if (4 * k + 3 < c + 3 && 4 * k + q < c) x[k] = fma(-xc, s.A[c][4 * k + q], x[k]);
+  }
+  if (valid) {
+#pragma unroll
+    for (int k = 0; k < kDenseTile / 4; ++k) {
+      const int c = 4 * k + q;
+      if (c < nb) mrow[c] = x[k];
+    }
+  }
+}
+
+// Phase B: M_IK -= X_IJ L_JK (16 x 16 threads, 4 x 4 outputs each).
+__device__ __forceinline__ void dense_trsm_update(double* __restrict__ M, const double* __restrict__ L, long long n,
+                                                  int I, int J, int K, DenseTrsmSmem& s) {
+  const long long oi = (long long)I * kDenseTile, oj = (long long)J * kDenseTile, ok = (long long)K * kDenseTile;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  __syncthreads();
+  for (int e = threadIdx.x; e < kDenseTile * kDenseTile; e += kDenseThreads) {
+    const int r = e >> 6, c = e & 63;
+    s.A[c][r] = (oi + r < n && oj + c < n) ? M[(oi + r) * n + oj + c] : 0.0;  // X_IJ, k-major
+    s.B[r][c] = (oj + r < n && ok + c < n) ? L[(oj + r) * n + ok + c] : 0.0;  // L_JK
+  }
+  __syncthreads();
+  double acc[4][4] = {};
+#pragma unroll 8
+  for (int m = 0; m < kDenseTile; ++m) {
+    const double2 a01 = *reinterpret_cast<const double2*>(&s.A[m][ty * 4]);
+    const double2 a23 = *reinterpret_cast<const double2*>(&s.A[m][ty * 4 + 2]);
+    const double2 b01 = *reinterpret_cast<const double2*>(&s.B[m][tx * 4]);
+    const double2 b23 = *reinterpret_cast<const double2*>(&s.B[m][tx * 4 + 2]);
+    const double a[4] = {a01.x, a01.y, a23.x, a23.y}, b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const long long r = oi + ty * 4 + u;
+    if (r >= n) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const long long c = ok + tx * 4 + v;
+      if (c < n) M[r * n + c] -= acc[u][v];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kDenseThreads) dense_trsm_kernel(double* __restrict__ M, const double* __restrict__ L,
+                                                                   long long n, DeviceStatus* st,
+                                                                   unsigned long long timeout_ns) {
+  extern __shared__ __align__(16) unsigned char trsm_smem[];
+  DenseTrsmSmem& s = *reinterpret_cast<DenseTrsmSmem*>(trsm_smem);
+  const int nt = (int)((n + kDenseTile - 1) / kDenseTile);
+  for (int J = nt - 1; J >= 0; --J) {
+    for (int I = blockIdx.x; I < nt; I += gridDim.x) dense_trsm_diag(M, L, n, I, J, s);
+    if (J == 0) break;
+    if (!dense_grid_barrier(st, timeout_ns)) return;
+    const int tiles = nt * J;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) dense_trsm_update(M, L, n, t / J, J, t % J, s);
+    if (!dense_grid_barrier(st, timeout_ns)) return;
+  }
+}
+
+inline cudaError_t launch_dense_trsm(double* M, const double* L, long long n, DeviceStatus* st,
+                                     unsigned long long timeout_ns, cudaStream_t s) {
+  auto kern = dense_trsm_kernel;
+  const size_t smem = sizeof(DenseTrsmSmem);
+  cudaError_t e = allow_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const long long nt = (n + kDenseTile - 1) / kDenseTile;
+  long long want = nt * (nt - 1);
+  if (want < nt) want = nt;
+  const int cap = persistent_grid(kern, kDenseThreads, smem, 0);
+  const int grid = (int)(want < cap ? want : cap);
+  void* params[] = {&M, const_cast<double**>(&L), &n, &st, &timeout_ns};
+  ggp::count_launch();
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(kDenseThreads), params,
+                                     smem, s);
+}
+
 }  // namespace ggp

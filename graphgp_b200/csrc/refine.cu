@@ -635,7 +635,7 @@ size_t vjp_extra_bytes(long long n, long long n0, int k, int nb, int tbytes) {
   Carver c(nullptr);
   c.take((size_t)tbytes * n);                                          // vbar
   c.take(sizeof(double) * (size_t)(kVjpMaxGrid + kRootHistGrid) * nb);  // bracket partials
-  for (int b = 0; b < 3; ++b) c.take(sizeof(double) * (size_t)n0 * n0);  // L^T, Q -> X, X^T -> Kbar^T
+  for (int b = 0; b < 2; ++b) c.take(sizeof(double) * (size_t)n0 * n0);  // Q -> X, X^T -> Kbar^T
   return c.off;
 }
 
@@ -662,7 +662,6 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
   Carver c(ws.extra);
   T* vbar = (T*)c.take(sizeof(T) * (size_t)n);
   double* partials = (double*)c.take(sizeof(double) * (size_t)(kVjpMaxGrid + kRootHistGrid) * nb);
-  double* LT = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
   double* X = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
   double* XT = (double*)c.take(sizeof(double) * (size_t)n0 * n0);
   if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
@@ -711,11 +710,14 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
   const double* L0 = ws.dense;
   double* y = ws.dense_x;
   (ggp::count_launch(), root_y_kernel<T><<<grid_for(n0 * 32), 256, 0, s>>>(L0, n0, vbar, xi, perm, y, out_grad_xi));
-  (ggp::count_launch(), transpose_kernel<<<grid_for(n0 * n0), 256, 0, s>>>(L0, n0, LT));
   (ggp::count_launch(), root_q_kernel<T><<<grid_for(n0 * n0), 256, 0, s>>>(y, xi, perm, n0, g_logdet, X));
-  (ggp::count_launch(), row_solve_kernel<<<grid_for(n0 * 32), 256, 0, s>>>(X, LT, n0, 1));
+  // X <- Q L^-1; X^T <- X^T L^-1 = L^-T Q^T L^-1 = Kbar0^T (blocked cooperative solves; L0 is zero above the
+  // diagonal)
+  cudaError_t te = launch_dense_trsm(X, L0, n0, ws.status, 10000000000ull, s);
+  if (te != cudaSuccess) return cuda_status(te);
   (ggp::count_launch(), transpose_kernel<<<grid_for(n0 * n0), 256, 0, s>>>(X, n0, XT));
-  (ggp::count_launch(), row_solve_kernel<<<grid_for(n0 * 32), 256, 0, s>>>(XT, LT, n0, 0));
+  te = launch_dense_trsm(XT, L0, n0, ws.status, 10000000000ull, s);
+  if (te != cudaSuccess) return cuda_status(te);
   const size_t hsmem = sizeof(double) * (size_t)nb;
   allow_smem(root_hist_kernel<T>, hsmem);
   (ggp::count_launch(), root_hist_kernel<T><<<kRootHistGrid, 256, hsmem, s>>>(XT, points, n0, d, ws.table, nb,

@@ -226,27 +226,6 @@ __global__ void root_q_kernel(const double* __restrict__ y, const T* __restrict_
   }
 }
 
-// In place, one warp per row r: M[r][:] <- M[r][:] L^-1 (solve X L = M), with LT = L^T. Rows of a lower
-// triangular M stay lower triangular, so those start at the diagonal.
-__global__ void row_solve_kernel(double* __restrict__ M, const double* __restrict__ LT, long long n, int lower) {
-  const int lane = threadIdx.x & 31;
-  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n;
-       r += ((long long)gridDim.x * blockDim.x) >> 5) {
-    double* mr = M + r * n;
-    const long long jstart = lower ? r : n - 1;
-    const long long kend = lower ? r : n - 1;
-    for (long long j = jstart; j >= 0; --j) {
-      const double* lj = LT + j * n;
-      double s = 0.0;
-      for (long long kk = j + 1 + lane; kk <= kend; kk += 32) s = fma(mr[kk], lj[kk], s);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) mr[j] = (mr[j] - s) / lj[j];
-      __syncwarp();
-    }
-  }
-}
-
 // Kbar^T entries (row b, column a) = Kbar[a][b] at r_ab -> table brackets; per-block histogram.
 template <typename T>
 __global__ void root_hist_kernel(const double* __restrict__ KbarT, const T* __restrict__ points, long long n0, int d,

@@ -24,7 +24,8 @@ def _t(x, dev, dtype=None):
 
 
 CASES = [(2000, 2, 100, 10, "rbf", 0.0), (2500, 3, 128, 16, "matern", 0.7), (1500, 2, 64, 20, "rbf", -1.3),
-         (1200, 3, 64, 7, "matern", 0.0)]
+         (1200, 3, 64, 7, "matern", 0.0),
+         (3000, 2, 300, 10, "rbf", 0.4)]  # a dense root of five 64-row tiles, the last one ragged
 
 
 def _table(name):
