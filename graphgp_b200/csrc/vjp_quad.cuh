@@ -170,25 +170,7 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
         }
       }
       __syncwarp();
-      {  // pair covariances, dealt p = g, g+4, ...
-        int i = 1, j = g;
-        while (j >= i) { j -= i; ++i; }
-        for (int pp = g; pp < SM::kPairs; pp += kQuad) {
-          T a = T(0);
-          if (!(PAD && ((i < K && i >= kk) || j >= kk))) {
-            T pi[D], pj[D];
-#pragma unroll
-            for (int c = 0; c < D; ++c) {
-              pi[c] = crd[i * SM::kPointStride + c];
-              pj[c] = crd[j * SM::kPointStride + c];
-            }
-            a = tab(point_distance<T, D>(pi, pj));
-          }
-          tri[pp] = a;
-          j += kQuad;
-          while (j >= i && i <= K) { j -= i; ++i; }
-        }
-      }
+      quad_pairs<T, K, D, PAD>(crd, tri, g, kk, tab);  // pair covariances, dealt p = g, g+4, ...
       __syncwarp();
       T wmine[NT], amine[NT], var;
       quad_factor_wa<T, K, NT>(tri, val, g, src0, c0, wmine, amine, var);
@@ -251,31 +233,32 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
       dpart = quad_sum(dpart);
       if (active) {
         if (g == 0) hist_add(hist, j0, dpart + 0.5 * sb * is, (double)t0, v.nb);
-        int i = 1, j = g;
-        while (j >= i) { j -= i; ++i; }
-        for (int pp = g; pp < SM::kPairs; pp += kQuad) {
-          if (!(PAD && ((i < K && i >= kk) || j >= kk))) {
-            T pi[D], pj[D];
-#pragma unroll
-            for (int c = 0; c < D; ++c) {
-              pi[c] = crd[i * SM::kPointStride + c];
-              pj[c] = crd[j * SM::kPointStride + c];
-            }
-            int jb;
-            T tt;
-            locate(tab, point_distance<T, D>(pi, pj), jb, tt);
-            const double wj = (double)tri[j], aj = (double)tri[K + j];
-            double cij;
-            if (i < K) {
-              const double wi = (double)tri[i], ai = (double)tri[K + i];
-              cij = -mb * (wi * aj + wj * ai) + sb * wi * wj * is;
-            } else {
-              cij = mb * aj - sb * wj * is;  // (neighbour j, self)
-            }
-            hist_add(hist, jb, cij, (double)tt, v.nb);
+        // pair 4 st + g from the warp-uniform pair table (as in quad_pairs), two steps in flight; the
+        // coefficient in the working precision, accumulated in FP64
+        constexpr int kSteps = (SM::kPairs + kQuad - 1) / kQuad;
+        const unsigned sel = 0x4440u | (unsigned)g;
+        const T tm = (T)mb, ts = (T)(sb * is);
+#pragma unroll kQuadPairUnroll
+        for (int st = 0; st < kSteps; ++st) {
+          if (SM::kPairs % kQuad != 0 && kQuad * st + g >= SM::kPairs) continue;
+          const uint2 ij = kQuadPairs.step[st];
+          const int i = (int)__byte_perm(ij.x, 0u, sel), j = (int)__byte_perm(ij.y, 0u, sel);
+          if (PAD && ((i < K && i >= kk) || j >= kk)) continue;
+          T pi[D], pj[D];
+          quad_load_slot<T, D>(crd + i * SM::kPointStride, pi);
+          quad_load_slot<T, D>(crd + j * SM::kPointStride, pj);
+          int jb;
+          T tt;
+          locate(tab, point_distance<T, D>(pi, pj), jb, tt);
+          const T wj = tri[j], aj = tri[K + j];
+          T cij;
+          if (i < K) {
+            const T wi = tri[i], ai = tri[K + i];
+            cij = -tm * (wi * aj + wj * ai) + ts * wi * wj;
+          } else {
+            cij = tm * aj - ts * wj;  // (neighbour j, self)
           }
-          j += kQuad;
-          while (j >= i && i <= K) { j -= i; ++i; }
+          hist_add(hist, jb, (double)cij, (double)tt, v.nb);
         }
       }
       __syncwarp();  // the scratch is reused by the next sub-iteration
