@@ -37,7 +37,11 @@ struct DeviceStatus {
   unsigned int listed;         // rows the FP32 inverse / logdet left to the FP64 second pass
   unsigned int bar_count;      // grid barrier of the dense-root kernel: blocks arrived
   unsigned int bar_gen;        // grid barrier of the dense-root kernel: generation
-  unsigned int pad[54];        // keeps the struct at 256 bytes
+  unsigned int sample_rows;    // FP32 inverse, sampling pass: rows factored
+  unsigned int sample_listed;  // ... and rows among them below the FP64 threshold
+  unsigned int all_fp64;       // set when the sample says most rows go to FP64: the FP32 pass is skipped and the
+                               // second pass takes every row
+  unsigned int pad[51];        // keeps the struct at 256 bytes
 };
 static_assert(sizeof(DeviceStatus) == 256, "status block must be 256 bytes");
 

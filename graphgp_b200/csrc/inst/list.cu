@@ -57,6 +57,25 @@ cudaError_t launch_list_warp(const RefineParams<float>& p, bool logdet, cudaStre
 
 }  // namespace
 
+// After the FP32 inverse's sampling pass: every row goes to the FP64 pass when more than `share` of the sampled rows
+// fell below the threshold (the FP32 pass is then skipped; `listed` becomes n - n0), else the ordinary passes
+// follow. Resets the ticket the sampling pass used.
+__global__ void list_decide_kernel(DeviceStatus* st, long long rows, double share) {
+  const unsigned int sampled = st->sample_rows, below = st->sample_listed;
+  const bool all = sampled > 0 && (double)below > share * (double)sampled;
+  st->all_fp64 = all ? 1u : 0u;
+  if (all) {
+    st->listed = (unsigned int)rows;
+    atomicAdd(&st->fallback_count, (unsigned int)rows);
+  }
+  st->ticket = 0;
+}
+
+cudaError_t launch_list_decide(DeviceStatus* st, long long rows, double share, cudaStream_t s) {
+  (ggp::count_launch(), list_decide_kernel<<<1, 1, 0, s>>>(st, rows, share));
+  return cudaGetLastError();
+}
+
 bool list_supported(int k, int d, int nb) { return quad_list_supported(k, d, nb) || list_warp_supported(k, d); }
 
 cudaError_t launch_list(const RefineParams<float>& p, bool logdet, int nb, cudaStream_t s) {

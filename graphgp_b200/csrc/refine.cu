@@ -249,12 +249,29 @@ RefineParams<T> make_params(const Workspace& ws, const T* points, long long n, i
   return p;
 }
 
+// FP32 inverse with a row list: a sampling pass factors every kInverseSampleStride-th chunk and counts the rows
+// below the threshold; when more than kAllFp64Share of them are, the FP32 pass is skipped and the FP64 pass takes
+// every row (the FP32 work on rows that end in FP64 anyway would be wasted: the FP64 pass costs about three FP32
+// passes, so the break-even share is near two thirds).
+constexpr int kInverseSampleStride = 32;
+constexpr double kAllFp64Share = 0.7;
+
 template <typename T>
 int run_cond(RefineParams<T> p, int mode, int nb, cudaStream_t s) {
   p.mode = mode;
   if (p.n_batches < 1 || p.n == p.n0) return GGP_OK;
+  cudaError_t e = cudaSuccess;
+  if constexpr (sizeof(T) == 4) {
+    if (mode == kInverse && p.fb_rows) {
+      RefineParams<T> q = p;
+      q.sample_stride = kInverseSampleStride;
+      e = dispatch<T>(q, kCond, nb, 0, s);
+      if (e == cudaSuccess) e = launch_list_decide(p.status, p.n - p.n0, kAllFp64Share, s);
+      stage_done("sampling pass", s);
+    }
+  }
   // generate waits batch on batch: -1 lets the launcher cap its width for the block size it picks
-  cudaError_t e = dispatch<T>(p, kCond, nb, mode == kGenerate ? -1 : 0, s);
+  if (e == cudaSuccess) e = dispatch<T>(p, kCond, nb, mode == kGenerate ? -1 : 0, s);
   stage_done("refinement", s);
   if constexpr (sizeof(T) == 4) {
     if (e == cudaSuccess && mode == kInverse && p.fb_rows) e = launch_list(p, false, nb, s);

@@ -26,6 +26,7 @@ __global__ void __launch_bounds__(128) refine_generic_kernel(RefineParams<T> p, 
   __shared__ long long s_row;
   __shared__ int s_ok;
   __shared__ double s_red[4];
+  if (p.sample_stride > 0) return;  // the inverse's sampling pass is for the FP32 kernels (this one lists nothing)
   const int k = p.k, d = p.d;
   const int n = (mode == 2) ? k + 1 : k + 2;  // matrix rows
   double* A = reinterpret_cast<double*>(smem);

@@ -37,6 +37,8 @@ struct RefineParams {
   int* fb_rows;             // inverse / logdet: rows below tau are listed here (count in status->listed) for the
                             // FP64 second pass instead of being re-conditioned in place; or null
   int table_smem;           // bytes of dynamic shared memory taken by the staged table (256-aligned)
+  int sample_stride;        // FP32 inverse with a row list: > 0 runs the sampling pass over every sample_stride-th
+                            // chunk (factor and count only); 0 is the ordinary pass
   unsigned long long timeout_ns;
 };
 
@@ -109,6 +111,29 @@ __device__ __forceinline__ void load_point(const T* __restrict__ points, long lo
 
 template <typename T>
 __device__ __forceinline__ void atomic_flag(unsigned int* f) { atomicOr(f, 1u); }
+
+// The FP32 inverse's pass over its rows is skipped when the sampling pass decided that most rows go to FP64.
+template <typename T>
+__device__ __forceinline__ bool skip_fp32_pass(const RefineParams<T>& p) {
+  return p.fb_rows != nullptr && p.sample_stride == 0 && ld_relaxed(reinterpret_cast<const int*>(&p.status->all_fp64)) != 0;
+}
+
+// Sampling pass: one factored row and whether it falls below the threshold.
+template <typename T>
+__device__ __forceinline__ void sample_row(const RefineParams<T>& p, bool below) {
+  atomicAdd(&p.status->sample_rows, 1u);
+  if (below) atomicAdd(&p.status->sample_listed, 1u);
+}
+
+// Chunks of a (possibly sampling) pass over `total` chunks, and the chunk a ticket stands for.
+template <typename T>
+__device__ __forceinline__ unsigned int pass_chunks(const RefineParams<T>& p, unsigned int total) {
+  return p.sample_stride > 0 ? (total + (unsigned int)p.sample_stride - 1u) / (unsigned int)p.sample_stride : total;
+}
+template <typename T>
+__device__ __forceinline__ unsigned int pass_chunk(const RefineParams<T>& p, unsigned int t) {
+  return p.sample_stride > 0 ? t * (unsigned int)p.sample_stride : t;
+}
 
 // Append a refined row to the FP64 second pass's list (inverse / logdet). The list holds n - n0 rows, one per
 // refined row; a slot past the end (a row listed twice) is refused and reported instead of written.

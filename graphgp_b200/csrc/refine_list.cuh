@@ -42,7 +42,9 @@ __global__ void __launch_bounds__(256) refine_list_kernel(RefineParams<float> p)
   T* crd = scratch + q * SM::kPerPoint;
   T* tri = crd + (K + 1) * SM::kPointStride;
   const int kk = p.k;
-  // the first pass has finished (stream order): the list length is final
+  // the first pass has finished (stream order): the list length is final; with all_fp64 the list is every row
+  // (the first pass was skipped) and `listed` holds n - n0
+  const bool all = ld_relaxed(reinterpret_cast<const int*>(&p.status->all_fp64)) != 0;
   unsigned int count = (unsigned int)ld_relaxed(reinterpret_cast<const int*>(&p.status->listed));
   if ((long long)count > p.n - p.n0) count = (unsigned int)(p.n - p.n0);  // list_row refused the excess
   const unsigned int chunks = (count + 7u) / 8u;
@@ -52,7 +54,7 @@ __global__ void __launch_bounds__(256) refine_list_kernel(RefineParams<float> p)
     if (t >= chunks) break;
     const unsigned int e = t * 8u + (unsigned int)q;
     const bool active = e < count;
-    long long row = active ? (long long)__ldg(p.fb_rows + e) : p.n0;
+    long long row = active ? (all ? p.n0 + (long long)e : (long long)__ldg(p.fb_rows + e)) : p.n0;
     if (!GGP_CHECK(row >= p.n0 && row < p.n, 202, row, e) || row < p.n0 || row >= p.n) row = p.n0;
     const long long r0 = row - p.n0;
     int ids[NT];
@@ -147,13 +149,14 @@ __global__ void __launch_bounds__(kListWarpBlock) refine_list_warp_kernel(Refine
   int* ids = reinterpret_cast<int*>(crd + (k + 1) * d);
   const TableView<double> tab = global_table_view<double>(p.tb);
   const double c0 = p.tb.desc->c0;
+  const bool all = ld_relaxed(reinterpret_cast<const int*>(&p.status->all_fp64)) != 0;  // every row, in order
   unsigned int count = (unsigned int)ld_relaxed(reinterpret_cast<const int*>(&p.status->listed));
   if ((long long)count > p.n - p.n0) count = (unsigned int)(p.n - p.n0);
   double acc_logdet = 0.0;
   for (;;) {
     const unsigned int t = warp_ticket(&p.status->ticket2);
     if (t >= count) break;
-    long long row = (long long)__ldg(p.fb_rows + t);
+    long long row = all ? p.n0 + (long long)t : (long long)__ldg(p.fb_rows + t);
     if (!GGP_CHECK(row >= p.n0 && row < p.n, 204, row, t) || row < p.n0 || row >= p.n) row = p.n0;
     const long long r0 = row - p.n0;
     for (int m = lane; m < k; m += 32) {
@@ -257,6 +260,10 @@ inline int list_k(int k) { return k <= 8 ? 8 : (k <= 16 ? 16 : 20); }
 // True when the FP32 inverse / logdet of this shape can leave its ill-conditioned points to a list pass (the quad
 // list kernel for k <= kListMaxK and d in {2, 3}, else the warp-per-point kernel for k <= kListWarpMaxK).
 bool list_supported(int k, int d, int nb);
+
+// After the FP32 inverse's sampling pass (RefineParams::sample_stride): every row goes to the FP64 pass when more
+// than `share` of the sampled rows fell below the threshold (inst/list.cu, list_decide_kernel).
+cudaError_t launch_list_decide(DeviceStatus* st, long long rows, double share, cudaStream_t s);
 
 // The FP64 list pass after an FP32 inverse (logdet = false) or log-determinant pass on the same stream.
 cudaError_t launch_list(const RefineParams<float>& p, bool logdet, int nb, cudaStream_t s);

@@ -302,6 +302,9 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
   constexpr int NT = QuadRows<K>::NT;
   extern __shared__ __align__(32) unsigned char smem[];
   __shared__ double s_part[4];
+  if constexpr (MODE == kOpInverse) {
+    if (skip_fp32_pass(p)) return;  // block-uniform: every row goes to the FP64 pass
+  }
   const TableView<T> tab = stage_table<T>(p.tb, smem);
   const T c0 = (T)p.tb.desc->c0;
   const int lane = threadIdx.x & 31;
@@ -312,9 +315,13 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
+  // the inverse's sampling pass takes every sample_stride-th chunk (constant false elsewhere)
+  const bool sampling = MODE == kOpInverse && p.sample_stride > 0;
+  const unsigned int chunks = MODE == kOpInverse ? pass_chunks(p, total) : total;
   for (;;) {
-    const unsigned int t = warp_ticket(&p.status->ticket);
-    if (t >= total) break;
+    const unsigned int tk = warp_ticket(&p.status->ticket);
+    if (tk >= chunks) break;
+    const unsigned int t = MODE == kOpInverse ? pass_chunk(p, tk) : tk;
     const int b = find_batch(p.chunk_prefix, p.n_batches, t);
     long long bstart = (long long)__ldg(p.offsets + b);
     bstart = bstart < p.n0 ? p.n0 : bstart;
@@ -345,7 +352,8 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
       if (active && g == 0) {
-        if (defer) list_row(p, row);
+        if (sampling) sample_row(p, fb);
+        else if (defer) list_row(p, row);
         else quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
       }
     }
@@ -532,6 +540,9 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
   using SM = QuadSmem<K, D>;
   extern __shared__ __align__(32) unsigned char smem[];
   __shared__ double s_part[Quad2Block<T>::kMax / 32];
+  if constexpr (MODE == kOpInverse) {
+    if (skip_fp32_pass(p)) return;  // block-uniform: every row goes to the FP64 pass
+  }
   // shared memory: table | per-warp point scratch (8 points per warp)
   const TableView<T> tab = stage_table<T>(p.tb, smem);
   const int warp = threadIdx.x >> 5;
@@ -547,9 +558,13 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
+  // the inverse's sampling pass takes every sample_stride-th chunk (constant false elsewhere)
+  const bool sampling = MODE == kOpInverse && p.sample_stride > 0;
+  const unsigned int chunks = MODE == kOpInverse ? pass_chunks(p, total) : total;
   for (;;) {
-    const unsigned int t = warp_ticket(&p.status->ticket);
-    if (t >= total) break;
+    const unsigned int tk = warp_ticket(&p.status->ticket);
+    if (tk >= chunks) break;
+    const unsigned int t = MODE == kOpInverse ? pass_chunk(p, tk) : tk;
     const int b = find_batch(p.chunk_prefix, p.n_batches, t);
     long long bstart = (long long)__ldg(p.offsets + b);
     bstart = bstart < p.n0 ? p.n0 : bstart;
@@ -594,7 +609,8 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
       if (active && g == 0) {
-        if (defer) list_row(p, row);  // constant false in the generate instantiation
+        if (sampling) sample_row(p, fb);
+        else if (defer) list_row(p, row);  // constant false in the generate instantiation
         else quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
       }
     }

@@ -107,6 +107,9 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
   constexpr int NA = tri_at(K, K) + 1;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double s_part[kTppBlock / 32];
+  if constexpr (MODE == kOpInverse) {
+    if (skip_fp32_pass(p)) return;  // block-uniform: every row goes to the FP64 pass
+  }
   const TppTable tab = stage_table_sentinel(p.tb, smem);
   const float c0 = (float)p.tb.desc->c0;
   const float inv_c0 = 1.f / c0;
@@ -114,15 +117,19 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
   const int kk = p.k;
   constexpr bool gen = MODE == kOpGenerate;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
+  // the inverse's sampling pass takes every sample_stride-th chunk (constant false elsewhere)
+  const bool sampling = MODE == kOpInverse && p.sample_stride > 0;
+  const unsigned int chunks = MODE == kOpInverse ? pass_chunks(p, total) : total;
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
   for (;;) {
     unsigned int t0 = 0;
     if (lane == 0) t0 = atomicAdd(&p.status->ticket, 4u);
     t0 = __shfl_sync(0xffffffffu, t0, 0);
-    if (t0 >= total) break;
-    const unsigned int t = t0 + (unsigned int)(lane >> 3);
-    if (t >= total) continue;
+    if (t0 >= chunks) break;
+    const unsigned int tl = t0 + (unsigned int)(lane >> 3);
+    if (tl >= chunks) continue;
+    const unsigned int t = MODE == kOpInverse ? pass_chunk(p, tl) : tl;
     const int b = find_batch(p.chunk_prefix, p.n_batches, t);
     long long bstart = (long long)__ldg(p.offsets + b);
     bstart = bstart < p.n0 ? p.n0 : bstart;
@@ -202,6 +209,10 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
     // list pass (inverse / logdet with p.fb_rows)
     const bool fb = !(mr >= (float)p.tau);
     if constexpr (!gen) {
+      if (sampling) {
+        sample_row(p, fb);
+        continue;
+      }
       if (fb && p.fb_rows) {
         list_row(p, row);
         continue;

@@ -229,3 +229,26 @@ def test_inverse_logdet_list_pass_k32(cuda_device, k, d):
     ld = float(gc.refine_logdet(*args))
     rld = orf.refine_logdet(g.points, g.neighbors, g.offsets, (bins, vals))
     assert abs(ld - rld) / abs(rld) < TOL32
+
+
+@pytest.mark.parametrize("tab,expect_all", [("rbf", 1), ("matern", 0)])
+def test_inverse_sampling_decides_fp64_share(cuda_device, tab, expect_all):
+    """The FP32 inverse samples every 32nd chunk first: with a smooth table most rows fall below the threshold and
+    every row is finished in FP64 (the FP32 pass is skipped); with a rough one the ordinary FP32 pass and row list
+    run. Both stay within the FP32 bar of the FP64 oracle."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    n, d, n0, k = 4000, 2, 128, 10
+    pts, g = oracle_graph(n, d, n0, k, seed=3)
+    bins, vals = as_inputs(_table(tab), np.float32)
+    f32 = torch.float32
+    v = np.random.default_rng(9).standard_normal(n).astype(np.float32)
+    i0, xi = gc.refine_inv(_t(g.points, cuda_device), _t(g.neighbors, cuda_device), g.offsets,
+                           _t(bins, cuda_device, f32), _t(vals, cuda_device, f32), _t(v, cuda_device, f32))
+    st = gc._tls.last_ws[:64].view(torch.int32).cpu().numpy()
+    assert int(st[12]) == expect_all  # DeviceStatus.all_fp64
+    if expect_all:
+        assert int(st[7]) == n - n0  # every row listed
+    ri0, rxi = orf.refine_inv(g.points, g.neighbors, g.offsets, (bins, vals), v)
+    assert rel_err(xi.cpu().numpy(), rxi) < TOL32
