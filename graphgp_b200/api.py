@@ -122,15 +122,15 @@ def generate_logdet(graph: Graph, covariance, *, cuda: bool = True):
 
 
 def generate_and_logdet(graph: Graph, covariance, xi, *, cuda: bool = True):
-    """``(generate(graph, covariance, xi), generate_logdet(graph, covariance))`` in one call; under autograd the
-    backward pass runs a single adjoint sweep for both outputs (a likelihood 0.5|v - y|^2 + logdet)."""
+    """``(generate(graph, covariance, xi), generate_logdet(graph, covariance))`` in one call (one forward pass in
+    FP32); under autograd the backward pass runs a single adjoint sweep for both outputs (a likelihood
+    0.5|v - y|^2 + logdet)."""
     _need_cuda(cuda)
     if _wants_grad(xi, covariance[1]):
         return _ag.generate_and_logdet(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0],
                                        covariance[1], xi)
-    return (_gc.generate(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0], covariance[1],
-                         xi),
-            _gc.generate_logdet(graph.points, graph.neighbors, graph.offsets, covariance[0], covariance[1]))
+    return _gc.generate_and_logdet(graph.points, graph.indices, graph.neighbors, graph.offsets, covariance[0],
+                                   covariance[1], xi)
 
 
 def generate_vjp(graph: Graph, covariance, xi, g_values, g_logdet: float = 0.0, *, values=None):

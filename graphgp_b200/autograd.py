@@ -72,14 +72,13 @@ class GenerateLogdetFn(torch.autograd.Function):
 
 
 class GenerateAndLogdetFn(torch.autograd.Function):
-    """(values, logdet) = (generate(xi, cov_vals), generate_logdet(cov_vals)) with one backward sweep for both
-    cotangents: the adjoint takes g_values and g_logdet together, so a loss that uses both (a Gaussian likelihood:
+    """(values, logdet) = (generate(xi, cov_vals), generate_logdet(cov_vals)), computed in one forward pass (FP32),
+    with one backward sweep for both cotangents: the adjoint takes g_values and g_logdet together, so a loss that uses both (a Gaussian likelihood:
     0.5 |values - y|^2 + logdet) costs one reverse pass instead of two."""
 
     @staticmethod
     def forward(ctx, xi, cov_vals, points, indices, neighbors, offsets, cov_bins, tau):
-        values = _gc.generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, tau=tau)
-        logdet = _gc.generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, tau=tau)
+        values, logdet = _gc.generate_and_logdet(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, tau=tau)
         ctx.save_for_backward(xi, cov_vals, values)
         ctx.graph = (points, indices, neighbors, offsets, cov_bins, tau)
         return values, logdet

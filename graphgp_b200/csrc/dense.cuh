@@ -29,7 +29,8 @@ struct DenseRootArgs {
   int d;
   TableBuffers tb;
   double* A;          // n0 x n0, row-major; the lower triangle ends as L
-  int mode;           // 0: out = L in, 1: out = L^-1 in, 2: *out_logdet = sum log L_ii
+  int mode;           // 0: out = L in (and *out_logdet = sum log L_ii when set), 1: out = L^-1 in,
+                      // 2: *out_logdet = sum log L_ii
   const T* in;        // (n0,), gathered through perm when perm is set
   const int* perm;    // graph row -> user index, or null
   T* out_graph;       // (n0,) graph order, or null
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(kDenseThreads) dense_root_kernel(DenseRootArgs
         if (a.out_user) a.out_user[a.perm ? a.perm[i] : i] = v;
       }
     }
-    return;
+    if (a.out_logdet == nullptr) return;  // else block 0 also writes sum log L_ii below (generate with logdet)
   }
   if (a.mode == 1) {  // out = L^-1 in: the last row of the augmented factor
     for (long long i = (long long)blockIdx.x * kDenseThreads + threadIdx.x; i < n;

@@ -463,6 +463,43 @@ int generate_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_
   return cuda_status(cudaGetLastError());
 }
 
+// generate and its log-determinant in one pass (FP32): the dense root writes sum log L_ii next to L xi, and the
+// refinement kernel (kOpGenerateLogdet) sums log std of every row into the per-block partials.
+int generate_and_logdet_f32_impl(const float* points, const int32_t* perm, int64_t n, int d, int64_t n0,
+                                 const int32_t* nbrs, int k, const int32_t* offsets, int n_offsets, const float* bins,
+                                 const float* vals, int nb, const float* xi, float* out, double* out_logdet,
+                                 double tau, uint64_t timeout_ns, void* wsp, size_t ws_bytes, cudaStream_t s) {
+  using T = float;
+  int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
+  if (rc) return rc;
+  if (n0 < 1 || n0 > n || !xi || !out || !out_logdet) return GGP_ERR_INVALID;
+  Workspace ws;
+  rc = carve_workspace(GGP_OP_GENERATE, n, d, n0, k, nb, n_offsets, sizeof(T), wsp, ws_bytes, &ws);
+  if (rc) return rc;
+  if ((rc = prologue<T>(ws, bins, vals, nb, offsets, n_offsets, n0, n, s))) return rc;
+  cudaMemsetAsync(ws.partials, 0, sizeof(double) * kMaxPartials, s);
+  T* vg = (T*)ws.values_graph;
+  (ggp::count_launch(), init_refine_values_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, nullptr, n0, n, offsets, n_offsets));
+  // L xi for the first n0 rows, and the dense log-determinant (refine.py:243-248) into dense_x[0]
+  if ((rc = dense_root<T>(ws, points, n0, d, 0, xi, perm, vg, out, ws.dense_x, s))) return rc;
+  RefineParams<T> p = make_params<T>(ws, points, n, d, nbrs, k, offsets, n_offsets, n0, tau, timeout_ns);
+  p.values = vg;
+  p.xi = xi;
+  p.perm = perm;
+  p.out_user = out;
+  p.gen_logdet = 1;
+  if (!perm) {
+    p.perm = nullptr;
+    p.out_user = nullptr;
+    p.xi = xi + n0;
+  }
+  if ((rc = run_cond<T>(p, kGenerate, nb, s))) return rc;
+  if (!perm) (ggp::count_launch(), copy_kernel<T><<<grid_for(n), 256, 0, s>>>(vg, out, n));
+  (ggp::count_launch(), poison_kernel<T><<<grid_for(n), 256, 0, s>>>(out, n, ws.status));
+  (ggp::count_launch(), sum_partials_kernel<<<1, 1024, 0, s>>>(ws.partials, kMaxPartials, ws.dense_x, out_logdet));
+  return cuda_status(cudaGetLastError());
+}
+
 template <typename T>
 int generate_inv_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                       const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* values,
@@ -601,6 +638,17 @@ int ggp_generate_f32(const float* points, const int32_t* indices, int64_t n, int
   return generate_impl<float>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals, n_bins,
                               xi, out_values, tau, timeout_ns, workspace, workspace_bytes, GGP_STREAM(stream));
 }
+
+int ggp_generate_and_logdet_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                                const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                                const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
+                                float* out_values, double* out_logdet, double tau, uint64_t timeout_ns,
+                                void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+  return generate_and_logdet_f32_impl(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
+                                      n_bins, xi, out_values, out_logdet, tau, timeout_ns, workspace, workspace_bytes,
+                                      GGP_STREAM(stream));
+}
+
 int ggp_generate_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                      const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const double* cov_bins,
                      const double* cov_vals, int n_bins, const double* xi, double* out_values, uint64_t timeout_ns,

@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(128) refine_generic_kernel(RefineParams<T> p, 
       double mean = 0.0;
       for (int w = 0; w < nw; ++w) mean += s_red[w];
       const double sd = A[packed_index(k, k)];
+      if (mode == 0 && p.gen_logdet) acc += log(sd);  // generate with the log-determinant
       if (mode == 0) {
         const T x = p.perm ? __ldg(p.xi + __ldg(p.perm + row)) : __ldg(p.xi + r0);
         T out = canonical((T)(mean + sd * (double)x));
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(128) refine_generic_kernel(RefineParams<T> p, 
       }
     }
   }
-  if (mode == 2 && tid == 0) {
+  if ((mode == 2 || (mode == 0 && p.gen_logdet)) && tid == 0) {
     if (acc != acc) atomicOr(&p.status->nan_seen, 1u);
     p.logdet_partials[blockIdx.x] = acc;
   }

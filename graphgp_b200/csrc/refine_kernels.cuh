@@ -10,7 +10,8 @@ namespace ggp {
 enum RefineMode : int { kGenerate = 0, kInverse = 1 };
 
 // Compile-time operation of a refinement kernel instantiation.
-enum RefineOp : int { kOpGenerate = 0, kOpInverse = 1, kOpLogdet = 2 };
+// kOpGenerateLogdet: generate that also sums log std of its rows into the log-determinant partials (FP32 only)
+enum RefineOp : int { kOpGenerate = 0, kOpInverse = 1, kOpLogdet = 2, kOpGenerateLogdet = 3 };
 
 template <typename T>
 struct RefineParams {
@@ -37,6 +38,7 @@ struct RefineParams {
   int* fb_rows;             // inverse / logdet: rows below tau are listed here (count in status->listed) for the
                             // FP64 second pass instead of being re-conditioned in place; or null
   int table_smem;           // bytes of dynamic shared memory taken by the staged table (256-aligned)
+  int gen_logdet;           // generate: also sum log std of every row into logdet_partials (one per block)
   int sample_stride;        // FP32 inverse with a row list: > 0 runs the sampling pass over every sample_stride-th
                             // chunk (factor and count only); 0 is the ordinary pass
   unsigned long long timeout_ns;

@@ -9,6 +9,10 @@ namespace ggp {
 
 enum KernelKind { kCond = 0, kLogdet = 1 };
 
+// The generate-with-log-determinant operation exists for FP32 only (FP64 callers take two passes); for double this
+// names the plain generate instantiation, so no kernel is compiled twice.
+template <typename T> struct GenLogdetOp { static constexpr int value = sizeof(T) == 4 ? kOpGenerateLogdet : kOpGenerate; };
+
 template <typename T, int K, int D, bool PAD>
 cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_blocks, cudaStream_t s);
 
@@ -32,8 +36,9 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
     const int block = (int)warps * 32;
     const size_t smem = q.table_smem + per_warp * warps;
     auto kern = (kind != kCond) ? refine_quad2_kernel<T, K, D, PAD, kOpLogdet>
-                : (p.mode == kGenerate ? refine_quad2_kernel<T, K, D, PAD, kOpGenerate>
-                                       : refine_quad2_kernel<T, K, D, PAD, kOpInverse>);
+                : (p.mode != kGenerate ? refine_quad2_kernel<T, K, D, PAD, kOpInverse>
+                   : (p.gen_logdet ? refine_quad2_kernel<T, K, D, PAD, GenLogdetOp<T>::value>
+                                   : refine_quad2_kernel<T, K, D, PAD, kOpGenerate>));
     cudaError_t e = allow_smem(kern, smem);
     if (e != cudaSuccess) return e;
     if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, block / 32);
@@ -45,8 +50,9 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
   const size_t smem = table_smem_bytes<T>(nb);
   if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, 4);
   auto kern = (kind != kCond) ? refine_quad_kernel<T, K, D, PAD, kOpLogdet>
-              : (p.mode == kGenerate ? refine_quad_kernel<T, K, D, PAD, kOpGenerate>
-                                     : refine_quad_kernel<T, K, D, PAD, kOpInverse>);
+              : (p.mode != kGenerate ? refine_quad_kernel<T, K, D, PAD, kOpInverse>
+                 : (p.gen_logdet ? refine_quad_kernel<T, K, D, PAD, GenLogdetOp<T>::value>
+                                 : refine_quad_kernel<T, K, D, PAD, kOpGenerate>));
   allow_smem(kern, smem);
   const int grid = persistent_grid(kern, 128, smem, max_blocks);
   (ggp::count_launch(), kern<<<grid, 128, smem, s>>>(p));

@@ -246,7 +246,7 @@ __device__ __forceinline__ void quad_refactor_f64(const RefineParams<T>& p, long
 
 // Finish one point in lane 0 of its quad: the FP64 mean of a re-conditioned point, then the output (value,
 // xi) or the logdet partial.
-template <typename T, int K, int D, bool LOGDET>
+template <typename T, int K, int D, bool LOGDET, bool ADDLD = false>
 __device__ __forceinline__ void quad_finish(const RefineParams<T>& p, bool gen, long long row, bool ok, T mean, T var,
                                             bool fb, const double (&w64)[K], double vd64, double& acc_logdet) {
   const long long r0 = row - p.n0;
@@ -272,6 +272,11 @@ __device__ __forceinline__ void quad_finish(const RefineParams<T>& p, bool gen, 
     if (l != l) atomicOr(&p.status->nan_seen, 1u);
     acc_logdet += l;
     return;
+  }
+  if constexpr (ADDLD) {  // generate with the log-determinant: log std of this row
+    const double l = 0.5 * log(vd);
+    if (l != l) atomicOr(&p.status->nan_seen, 1u);
+    acc_logdet += l;
   }
   const T sd = (T)sqrt(vd);
   const T mu = (T)md;
@@ -311,7 +316,8 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
   const int g = lane & (kQuad - 1);
   const int q = lane >> 2;
   const int src0 = lane & ~(kQuad - 1);
-  constexpr bool gen = MODE == kOpGenerate;
+  constexpr bool gen = MODE == kOpGenerate || MODE == kOpGenerateLogdet;
+  constexpr bool GENLD = MODE == kOpGenerateLogdet;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
@@ -354,11 +360,11 @@ __global__ void __launch_bounds__(128) refine_quad_kernel(RefineParams<T> p) {
       if (active && g == 0) {
         if (sampling) sample_row(p, fb);
         else if (defer) list_row(p, row);
-        else quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
+        else quad_finish<T, K, D, LOGDET, GENLD>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
       }
     }
   }
-  if (LOGDET) {
+  if (LOGDET || GENLD) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc_logdet += __shfl_xor_sync(0xffffffffu, acc_logdet, o);
     if (lane == 0) s_part[threadIdx.x >> 5] = acc_logdet;
@@ -554,7 +560,8 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
   const int src0 = lane & ~(kQuad - 1);
   T* crd = scratch + q * SM::kPerPoint;                      // (K+1) x kPointStride
   T* tri = crd + (K + 1) * SM::kPointStride;                 // kPairs
-  constexpr bool gen = MODE == kOpGenerate;
+  constexpr bool gen = MODE == kOpGenerate || MODE == kOpGenerateLogdet;
+  constexpr bool GENLD = MODE == kOpGenerateLogdet;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
@@ -611,11 +618,11 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
       if (active && g == 0) {
         if (sampling) sample_row(p, fb);
         else if (defer) list_row(p, row);  // constant false in the generate instantiation
-        else quad_finish<T, K, D, LOGDET>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
+        else quad_finish<T, K, D, LOGDET, GENLD>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
       }
     }
   }
-  if (LOGDET) {
+  if (LOGDET || GENLD) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc_logdet += __shfl_xor_sync(0xffffffffu, acc_logdet, o);
     if (lane == 0) s_part[threadIdx.x >> 5] = acc_logdet;

@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
   const float inv_c0 = 1.f / c0;
   const int lane = threadIdx.x & 31;
   const int kk = p.k;
-  constexpr bool gen = MODE == kOpGenerate;
+  constexpr bool gen = MODE == kOpGenerate || MODE == kOpGenerateLogdet;
+  constexpr bool GENLD = MODE == kOpGenerateLogdet;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   // the inverse's sampling pass takes every sample_stride-th chunk (constant false elsewhere)
   const bool sampling = MODE == kOpInverse && p.sample_stride > 0;
@@ -230,11 +231,11 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
       vd = vd64;
       atomicAdd(&p.status->fallback_count, 1u);
     }
-    if (LOGDET) {
+    if (LOGDET || GENLD) {
       const double l = 0.5 * log(vd);
       if (l != l) atomicOr(&p.status->nan_seen, 1u);
       acc_logdet += l;
-      continue;
+      if (LOGDET) continue;
     }
     // neighbour values: in generate they may still be pending (the value itself is the ready flag); the ids are
     // read again rather than kept live through the factorisation
@@ -320,7 +321,7 @@ __global__ void __launch_bounds__(kTppBlock, GGP_TPP_MIN_BLOCKS) refine_tpp_kern
       }
     }
   }
-  if (LOGDET) {
+  if (LOGDET || GENLD) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc_logdet += __shfl_xor_sync(0xffffffffu, acc_logdet, o);
     if (lane == 0) s_part[threadIdx.x >> 5] = acc_logdet;
@@ -342,8 +343,9 @@ template <int K, int D, bool PAD>
 cudaError_t launch_tpp(const RefineParams<float>& p, int kind, int nb, int max_blocks, cudaStream_t s) {
   const size_t smem = tpp_table_smem(nb);
   auto kern = kind == 1 ? refine_tpp_kernel<K, D, PAD, kOpLogdet>
-              : (p.mode == kGenerate ? refine_tpp_kernel<K, D, PAD, kOpGenerate>
-                                     : refine_tpp_kernel<K, D, PAD, kOpInverse>);
+              : (p.mode != kGenerate ? refine_tpp_kernel<K, D, PAD, kOpInverse>
+                 : (p.gen_logdet ? refine_tpp_kernel<K, D, PAD, kOpGenerateLogdet>
+                                 : refine_tpp_kernel<K, D, PAD, kOpGenerate>));
   cudaError_t e = allow_smem(kern, smem);
   if (e != cudaSuccess) return e;
   if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, kTppBlock / 32, 4);

@@ -347,6 +347,28 @@ def generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau
     return out
 
 
+def generate_and_logdet(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau=None, timeout_ns=0):
+    """``generate`` and ``generate_logdet`` of the same table -> (values (N,), logdet (0-d float64)). In FP32 one
+    pass computes both (``ggp_generate_and_logdet_f32``); in FP64 the two calls run one after the other."""
+    if _suffix(_cuda(points, "points").dtype) != "f32":
+        return (generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, tau=tau, timeout_ns=timeout_ns),
+                generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, tau=tau))
+    points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
+    bins, vals = _table(cov_bins, cov_vals, points.dtype)
+    xi = _cuda(xi, "xi", points.dtype)
+    if xi.numel() != n:
+        raise ValueError("Length of xi must match number of points in graph.")
+    idx = None if indices is None else _ids(indices, "indices")
+    out = torch.empty(n, dtype=points.dtype, device=points.device)
+    ld = torch.empty((), dtype=torch.float64, device=points.device)
+    ws = _workspace("GENERATE", n, d, n0, k, len(bins), len(offs), points.element_size(), points.device)
+    rc = _lib.load().ggp_generate_and_logdet_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
+                                                 _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(out), _ptr(ld),
+                                                 _tau(tau), int(timeout_ns), _ptr(ws), ws.numel(), _stream())
+    _lib.check(rc, "generate_and_logdet")
+    return out, ld
+
+
 def generate_inv(points, indices, neighbors, offsets, cov_bins, cov_vals, values, *, tau=None):
     """Whole ``generate_inv`` (reference refine.py:162-183) in one device call."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)

@@ -235,6 +235,14 @@ int ggp_generate_f64(const double* points, const int32_t* indices, int64_t n, in
                      int k, const int32_t* offsets, int n_offsets, const double* cov_bins, const double* cov_vals,
                      int n_bins, const double* xi, double* out_values, uint64_t timeout_ns, void* workspace,
                      size_t workspace_bytes, ggp_stream_t stream);
+/* generate and generate_logdet of the same table in one pass (FP32; no counterpart in the reference, where a    */
+/* loss using both calls each): values as ggp_generate_f32, and the log-determinant (as ggp_generate_logdet_f32, */
+/* device FP64) summed from the same factorisations. Workspace: ggp_workspace_size(GGP_OP_GENERATE, ...).       */
+int ggp_generate_and_logdet_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                                const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                                const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
+                                float* out_values, double* out_logdet, double tau, uint64_t timeout_ns,
+                                void* workspace, size_t workspace_bytes, ggp_stream_t stream);
 int ggp_generate_inv_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                          const float* cov_bins, const float* cov_vals, int n_bins, const float* values,

@@ -252,3 +252,26 @@ def test_inverse_sampling_decides_fp64_share(cuda_device, tab, expect_all):
         assert int(st[7]) == n - n0  # every row listed
     ri0, rxi = orf.refine_inv(g.points, g.neighbors, g.offsets, (bins, vals), v)
     assert rel_err(xi.cpu().numpy(), rxi) < TOL32
+
+
+@pytest.mark.parametrize("d,k", [(2, 10), (3, 16), (3, 32), (4, 8)])
+def test_generate_and_logdet_one_pass(cuda_device, d, k):
+    """generate_and_logdet (FP32, one pass: the dense root and the refinement kernel also sum the log-determinant)
+    gives generate's values bit for bit and generate_logdet's log-determinant to FP64 rounding, for the
+    one-thread-per-point (k <= 10), four-lane (k 16, 32) and generic (d = 4) kernels."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    n, n0 = 3000, 200
+    pts, g = oracle_graph(n, d, n0, k, seed=13)
+    bins, vals = as_inputs(rbf_table(), np.float32)
+    f32 = torch.float32
+    args = (_t(g.points, cuda_device), _t(g.indices, cuda_device), _t(g.neighbors, cuda_device), g.offsets,
+            _t(bins, cuda_device, f32), _t(vals, cuda_device, f32))
+    xi = _t(np.random.default_rng(1).standard_normal(n).astype(np.float32), cuda_device)
+    v, ld = gc.generate_and_logdet(*args, xi)
+    assert torch.equal(v, gc.generate(*args, xi))
+    ref = float(gc.generate_logdet(args[0], args[2], args[3], args[4], args[5]))
+    assert abs(float(ld) - ref) <= 1e-9 * abs(ref)
+    rld = orf.generate_logdet(g, (bins, vals))
+    assert abs(float(ld) - rld) / abs(rld) < TOL32
