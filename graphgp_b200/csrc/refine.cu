@@ -12,6 +12,7 @@
 #include "refine_list.cuh"
 #include "refine_tpp.cuh"
 #include "vjp.cuh"
+#include "vjp_warp.cuh"
 #include "vjp_quad.cuh"
 
 namespace ggp {
@@ -761,6 +762,26 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
     cudaError_t e = d == 2 ? vjp_quad_dispatch_k<T, 2>(v, k, kVjpMaxGrid, s) : vjp_quad_dispatch_k<T, 3>(v, k, kVjpMaxGrid, s);
     if (e == cudaSuccess) swept = true;
     else if (e != cudaErrorInvalidConfiguration) return cuda_status(e);
+  }
+  if (!swept && n > n0 && n_offsets > 1 && k <= kVjpMaxK) {
+    // one warp per point, as many warps per block (up to 16) as the table and histogram leave room for
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t hist_bytes = ((size_t)nb * sizeof(double) + 255) / 256 * 256;
+    const size_t per_warp = sizeof(T) * (size_t)vjp_warp_elems<T>(k, d);
+    long warps = ((long)optin - kSmemHeadroom - (long)v.r.table_smem - (long)hist_bytes) / (long)per_warp;
+    if (warps > 16) warps = 16;
+    if (warps >= 2) {
+      const size_t smem = v.r.table_smem + hist_bytes + per_warp * (size_t)warps;
+      auto kern = vjp_warp_kernel<T>;
+      cudaError_t e = allow_smem(kern, smem);
+      if (e != cudaSuccess) return cuda_status(e);
+      const int cap = dataflow_blocks(n, n0, n_offsets - 1, (int)warps);
+      const int grid = persistent_grid(kern, (int)warps * 32, smem, cap > 0 && cap < kVjpMaxGrid ? cap : kVjpMaxGrid);
+      (ggp::count_launch(), kern<<<grid, (int)warps * 32, smem, s>>>(v));
+      swept = true;
+    }
   }
   if (!swept && n > n0 && n_offsets > 1) {
     const size_t smem = v.r.table_smem + sizeof(double) * (size_t)nb;
