@@ -7,11 +7,11 @@
 // it factors each of the chunk's points: the covariances of [nbrs, self] from the table, a right-looking Cholesky
 // of [nbrs, self, v] (the neighbour values as a last row, so that the factorisation leaves z = L11^-1 v_N there),
 // sigma = L[k][k], and w = L11^-T l21, a = L11^-T z by backward substitution with lane m holding entry m. The
-// chunk's w, a, sigma, ids and coordinates wait in a per-warp buffer. The wait: every chunk of the later batches
-// finished (a chunk-granular completion counter; those chunks hold earlier tickets). On the chain: xibar = sigma
-// vbar and the scatter of w_m vbar into the neighbours' cotangents, then the chunk is counted. Off the chain: the
-// derivatives of (mean, sigma) with respect to every covariance entry into the block's FP64 histogram over the
-// table brackets.
+// chunk's w, a, sigma and ids wait in a per-warp buffer (coordinates are gathered again after the wait). The wait:
+// every chunk of the later batches finished (a chunk-granular completion counter; those chunks hold earlier
+// tickets). On the chain: xibar = sigma vbar and the scatter of w_m vbar into the neighbours' cotangents, then the
+// chunk is counted. Off the chain: the derivatives of (mean, sigma) with respect to every covariance entry into
+// the block's FP64 histogram over the table brackets.
 #pragma once
 
 #include "refine_quad.cuh"  // kQuadPairs: the (i, j) of flat pair index p = i(i-1)/2 + j
@@ -23,12 +23,12 @@ constexpr int kVjpWarpChunk = 8;  // rows per chunk (chunk_rows())
 
 __device__ __forceinline__ int vw_packed(int i, int j) { return i * (i + 1) / 2 + j; }
 
-// Elements of T per warp: the packed matrix of rows 0..k+1, and for the chunk's 8 points w, a, coordinates,
-// sigma and the neighbour ids (stored as T-sized slots), rounded up to 16 bytes.
+// Elements of T per warp: the packed matrix of rows 0..k+1, one point's coordinates, and for the chunk's 8 points
+// w, a, sigma and the neighbour ids (stored as T-sized slots), rounded up to 16 bytes.
 template <typename T>
 __host__ __device__ inline int vjp_warp_elems(int k, int d) {
   const int nr = k + 2;
-  const int n = nr * (nr + 1) / 2 + kVjpWarpChunk * (2 * k + (k + 1) * d + 1 + k);
+  const int n = nr * (nr + 1) / 2 + (k + 1) * d + kVjpWarpChunk * (2 * k + 1 + k);
   const int per16 = 16 / (int)sizeof(T);
   return (n + per16 - 1) / per16 * per16;
 }
@@ -36,18 +36,18 @@ __host__ __device__ inline int vjp_warp_elems(int k, int d) {
 template <typename T>
 struct VjpWarpScratch {
   T* A;     // packed rows 0..k+1
+  T* crd;   // [(k+1) d] of the point in hand, row k = the point itself
   T* W;     // [8][k]
   T* Aa;    // [8][k]
-  T* crd;   // [8][(k+1) d], row k = the point itself
   T* sig;   // [8]
   int* ids;  // [8][k] (in T-sized slots)
   __device__ VjpWarpScratch(T* base, int k, int d) {
     const int nr = k + 2;
     A = base;
-    W = A + nr * (nr + 1) / 2;
+    crd = A + nr * (nr + 1) / 2;
+    W = crd + (k + 1) * d;
     Aa = W + kVjpWarpChunk * k;
-    crd = Aa + kVjpWarpChunk * k;
-    sig = crd + kVjpWarpChunk * (k + 1) * d;
+    sig = Aa + kVjpWarpChunk * k;
     ids = reinterpret_cast<int*>(sig + kVjpWarpChunk);  // T-aligned, and T is at least int-sized
   }
 };
@@ -60,7 +60,7 @@ __device__ __forceinline__ void vjp_warp_factor(const RefineParams<T>& p, const 
   const int k = p.k, d = p.d, vr = k + 1;
   const long long r0 = row - p.n0;
   int* ids = S.ids + pt * k;
-  T* crd = S.crd + pt * (k + 1) * d;
+  T* crd = S.crd;
   for (int m = lane; m < k; m += 32) {
     int id = __ldg(p.nbrs + r0 * k + m);
     if (id < 0 || (long long)id >= bstart) {  // neighbours precede their point's batch
@@ -205,7 +205,14 @@ __global__ void __launch_bounds__(512) vjp_warp_kernel(VjpParams<T> v) {
       const double is = 1.0 / (double)sig;
       const T* W = S.W + pt * k;
       const T* Aa = S.Aa + pt * k;
-      const T* crd = S.crd + pt * (k + 1) * d;
+      T* crd = S.crd;  // the point's coordinates again (L2 hits; the previous point's reads are done)
+      __syncwarp();
+      for (int e = lane; e < (k + 1) * d; e += 32) {
+        const int i = e / d, c = e - i * d;
+        const long long pid = i < k ? (long long)S.ids[pt * k + i] : row;
+        crd[e] = __ldg(p.points + pid * d + c);
+      }
+      __syncwarp();
       double dpart = 0.0;
       for (int i = lane; i < k; i += 32) {
         const double wi = W[i], ai = Aa[i];
