@@ -177,20 +177,33 @@ __global__ void __launch_bounds__(kListWarpBlock) refine_list_warp_kernel(Refine
       }
     }
     __syncwarp();
-    for (int i = 0; i <= k; ++i) {
-      for (int j = lane; j <= i; j += 32) {
-        double v = c0;
-        if (j != i) {
+    // the k(k+1)/2 pairs (i, j), j < i <= k, dealt over the lanes (pair table of the quad kernels; k <= 32),
+    // else row by row
+    if (k <= kQuadPairMaxK) {
+      for (int e = lane; e < k * (k + 1) / 2; e += 32) {
+        const uint2 ij = kQuadPairs.step[e >> 2];
+        const int sh = 8 * (e & 3);
+        const int i = (int)((ij.x >> sh) & 0xffu), j = (int)((ij.y >> sh) & 0xffu);
+        double s2 = 0.0;
+        for (int c = 0; c < d; ++c) {
+          const double df = crd[i * d + c] - crd[j * d + c];
+          s2 = fma(df, df, s2);
+        }
+        A[list_packed(i, j)] = tab(sqrt(s2));
+      }
+    } else {
+      for (int i = 1; i <= k; ++i) {
+        for (int j = lane; j < i; j += 32) {
           double s2 = 0.0;
           for (int c = 0; c < d; ++c) {
             const double df = crd[i * d + c] - crd[j * d + c];
             s2 = fma(df, df, s2);
           }
-          v = tab(sqrt(s2));
+          A[list_packed(i, j)] = tab(sqrt(s2));
         }
-        A[list_packed(i, j)] = v;
       }
     }
+    for (int i = lane; i <= k; i += 32) A[list_packed(i, i)] = c0;
     __syncwarp();
     // right-looking Cholesky over columns 0..k; the value row (inverse) is updated like the others
     for (int j = 0; j <= k; ++j) {
@@ -198,10 +211,12 @@ __global__ void __launch_bounds__(kListWarpBlock) refine_list_warp_kernel(Refine
       for (int i = j + 1 + lane; i < nr; i += 32) A[list_packed(i, j)] /= djj;
       __syncwarp();
       if (lane == 0) A[list_packed(j, j)] = djj;
-      for (int i = j + 1; i < nr; ++i) {
+      __syncwarp();  // column j is scaled
+      for (int i = j + 1 + lane; i < nr; i += 32) {  // one lane per row
         const double lij = A[list_packed(i, j)];
         const int mmax = i <= k ? i : k;
-        for (int m = j + 1 + lane; m <= mmax; m += 32) A[list_packed(i, m)] -= lij * A[list_packed(m, j)];
+        double* ri = A + list_packed(i, 0);
+        for (int m = j + 1; m <= mmax; ++m) ri[m] = fma(-lij, A[list_packed(m, j)], ri[m]);
       }
       __syncwarp();
     }
