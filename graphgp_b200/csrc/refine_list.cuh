@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(256) refine_list_kernel(RefineParams<float> p)
   extern __shared__ __align__(32) unsigned char smem[];
   __shared__ double s_part[8];
   const TableView<double> tab = stage_table<double>(p.tb, smem);
-  GGP_CHECK((reinterpret_cast<uintptr_t>(smem) & 31) == 0, 201, reinterpret_cast<uintptr_t>(smem), p.table_smem);
+  (void)GGP_CHECK((reinterpret_cast<uintptr_t>(smem) & 31) == 0, 201, reinterpret_cast<uintptr_t>(smem), p.table_smem);
   const int warp = threadIdx.x >> 5;
   T* scratch = reinterpret_cast<T*>(smem + p.table_smem) + (size_t)warp * 8 * SM::kPerPoint;
   const T c0 = p.tb.desc->c0;
