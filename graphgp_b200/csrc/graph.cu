@@ -68,6 +68,7 @@ struct OrderWs {
   uint32_t* key[2];
   int* val[2];
   unsigned int* counts;
+  unsigned long long* span_sums;  // per-span totals of the counts' multi-block scan
   int* inv;
 };
 
@@ -80,8 +81,10 @@ static size_t order_ws_bytes(long long n, OrderWs* w, char* base) {
     if (w) { w->key[b] = k; w->val[b] = v; }
   }
   auto* cnt = (unsigned int*)c.take(sizeof(unsigned int) * (size_t)tiles * 256);
+  const long long spans = (tiles * 256 + kScanSpan - 1) / kScanSpan;
+  auto* ss = (unsigned long long*)c.take(sizeof(unsigned long long) * (size_t)spans);
   auto* inv = (int*)c.take(sizeof(int) * (size_t)n);
-  if (w) { w->counts = cnt; w->inv = inv; }
+  if (w) { w->counts = cnt; w->span_sums = ss; w->inv = inv; }
   return c.off;
 }
 
@@ -298,7 +301,13 @@ static int order_device(const T* points, const int* indices, const int* nbrs, co
   int cur = 0;
   for (int shift = 0; shift < bits; shift += 8) {
     (ggp::count_launch(), radix_hist_kernel<<<tiles, kSortThreads, 0, s>>>(w.key[cur], n, shift, w.counts, tiles));
-    (ggp::count_launch(), exclusive_scan_kernel<<<1, 1024, 0, s>>>(w.counts, (long long)tiles * 256));
+    {  // exclusive scan of the tile counts: span totals, their scan, the spans
+      const long long m = (long long)tiles * 256;
+      const int spans = (int)((m + kScanSpan - 1) / kScanSpan);
+      (ggp::count_launch(), scan_span_sums_kernel<<<spans, kScanThreads, 0, s>>>(w.counts, m, w.span_sums));
+      (ggp::count_launch(), exclusive_scan_u64_kernel<<<1, 1024, 0, s>>>(w.span_sums, spans));
+      (ggp::count_launch(), scan_span_apply_kernel<<<spans, kScanThreads, 0, s>>>(w.counts, m, w.span_sums));
+    }
     (ggp::count_launch(), radix_scatter_kernel<<<tiles, kSortThreads, 0, s>>>(w.key[cur], w.val[cur], w.key[cur ^ 1], w.val[cur ^ 1], n, shift,
                                                         w.counts, tiles));
     cur ^= 1;

@@ -108,14 +108,52 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t
 // Exclusive scan of `m` counters in one block (digit-major order gives each (digit, tile) its base).
 // In-place exclusive scan of m counts by one block of 1024 threads, 1024 consecutive entries per step (coalesced):
 // a warp-shuffle scan per warp, a scan of the 32 warp totals, and a running carry between steps.
-__global__ void __launch_bounds__(1024) exclusive_scan_kernel(unsigned int* __restrict__ a, long long m) {
+// Multi-block exclusive scan of m counts (the digit-major tile counts of one radix pass), kScanSpan elements per
+// block: block totals, an exclusive scan of the totals (exclusive_scan_u64_kernel, one block), then each block
+// scans its span from its total's prefix. The counts of one pass sum to n < 2^31, so every prefix fits in 32 bits.
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanSpan = kScanThreads * kScanItems;
+
+__device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v, unsigned long long* warp_sums) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) warp_sums[wid] = v;
+  __syncthreads();
+  unsigned long long t = 0;
+  if (wid == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  return t;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_span_sums_kernel(const unsigned int* __restrict__ a, long long m,
+                                                                     unsigned long long* __restrict__ sums) {
+  __shared__ unsigned long long warp_sums[32];
+  const long long base = (long long)blockIdx.x * kScanSpan;
+  unsigned long long v = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    const long long i = base + (long long)q * kScanThreads + threadIdx.x;
+    if (i < m) v += a[i];
+  }
+  const unsigned long long t = block_sum_u64(v, warp_sums);
+  if (threadIdx.x == 0) sums[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_span_apply_kernel(unsigned int* __restrict__ a, long long m,
+                                                                      const unsigned long long* __restrict__ prefix) {
   __shared__ unsigned long long warp_sums[32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  unsigned long long carry = 0;
-  for (long long base = 0; base < m; base += 1024) {
-    const long long i = base + threadIdx.x;
+  const long long base = (long long)blockIdx.x * kScanSpan;
+  unsigned long long carry = prefix[blockIdx.x];
+  for (int q = 0; q < kScanItems; ++q) {
+    const long long i = base + (long long)q * kScanThreads + threadIdx.x;
     const unsigned long long x = i < m ? a[i] : 0ull;
-    unsigned long long v = x;  // inclusive scan within the warp
+    unsigned long long v = x;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
@@ -139,6 +177,40 @@ __global__ void __launch_bounds__(1024) exclusive_scan_kernel(unsigned int* __re
     __syncthreads();  // warp_sums is rewritten in the next step
   }
 }
+
+// Exclusive scan in place of m 64-bit totals, one block.
+__global__ void __launch_bounds__(1024) exclusive_scan_u64_kernel(unsigned long long* __restrict__ a, long long m) {
+  __shared__ unsigned long long warp_sums[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned long long carry = 0;
+  for (long long base = 0; base < m; base += 1024) {
+    const long long i = base + threadIdx.x;
+    const unsigned long long x = i < m ? a[i] : 0ull;
+    unsigned long long v = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    if (lane == 31) warp_sums[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+      unsigned long long w = warp_sums[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const unsigned long long before = wid > 0 ? warp_sums[wid - 1] : 0ull;
+    if (i < m) a[i] = carry + before + v - x;
+    carry += warp_sums[31];
+    __syncthreads();
+  }
+}
+
 
 __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint32_t* __restrict__ kin,
                                                                      const int* __restrict__ vin,
