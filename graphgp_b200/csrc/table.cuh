@@ -104,9 +104,12 @@ __global__ void prepare_table_kernel(const TB* __restrict__ bins, const TB* __re
                                      TableBuffers tb) {
   __shared__ long long s_key_lo32, s_key_lo64;
   __shared__ int s_shift32, s_shift64, s_nh;
+  // sortedness, checked by the whole block
+  int sorted_part = 1;
+  for (int j = 1 + (int)threadIdx.x; j < nb; j += blockDim.x)
+    sorted_part &= ((double)bins[j - 1] <= (double)bins[j]) ? 1 : 0;
+  const int sorted = __syncthreads_and(sorted_part);
   if (threadIdx.x == 0) {
-    int sorted = 1;
-    for (int j = 1; j < nb; ++j) sorted &= ((double)bins[j - 1] <= (double)bins[j]) ? 1 : 0;
     // first strictly positive bin (bins[0] is normally exactly 0)
     int jp = 0;
     while (jp < nb - 1 && !((double)bins[jp] > 0.0)) ++jp;
