@@ -98,8 +98,10 @@ _SIGS = {
                               _P], _I),
     "ggp_wait_probe": ([_U64, C.POINTER(C.c_int), _P, _SZ, _P], _I),
     "ggp_fma_probe": ([_I, _I, _I, C.POINTER(C.c_double), _P, _SZ, _P], _I),
-    "ggp_generate_and_logdet_f32": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _D, _U64, _P, _SZ,
-                                     _P], _I),
+    "ggp_generate_and_logdet_f32": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P, _D, _U64,
+                                     _P, _SZ, _P], _I),
+    "ggp_generate_vjp_resid_f32": ([_P, _P, _I64, _I, _I64, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _D, _P, _P, _D,
+                                    _P, _SZ, _P], _I),
     "ggp_request_buffer_size": ([_I, _I64, _I, _I64, _I, _I, _I], _SZ),
     "ggp_request_f32": ([_I, _P, _I64, _I, _I64, _I, _P, _P, _I, _P, _P, _P, _D, _P, _SZ, _P], _I),
     "ggp_request_f64": ([_I, _P, _I64, _I, _I64, _I, _P, _P, _I, _P, _P, _P, _P, _SZ, _P], _I),

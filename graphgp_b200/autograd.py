@@ -11,7 +11,9 @@ reverse sweep on the device:
   backward returns d<g, values>/dxi (N,) and d<g, values>/dcov_vals (n_bins,).
 * ``GenerateLogdetFn``: logdet = generate_logdet(cov_vals) (FP64 0-d tensor); its backward returns
   g * dlogdet/dcov_vals through the same adjoint with a zero value cotangent.
-* ``GenerateAndLogdetFn``: both at once, with one adjoint sweep for both cotangents (a Gaussian likelihood).
+* ``GenerateAndLogdetFn``: both at once, with one adjoint sweep for both cotangents (a Gaussian likelihood). In
+  FP32 with 10 < k <= 20 and d in {2, 3} its forward also keeps each refined row's w, a and sigma (``RESIDUALS``),
+  which the backward sweep reads instead of refactorising the row.
 
 The graph (points, neighbours, offsets, indices) and the table's bins are constants: no gradient flows to them.
 This is the JAX ``custom_vjp`` that a ``jax.ffi`` host would register written for torch.
@@ -21,6 +23,10 @@ from __future__ import annotations
 import torch
 
 from . import graphgp_cuda as _gc
+
+# GenerateAndLogdetFn keeps each refined row's w, a and sigma from its forward pass ((2k + 1) FP32 per row) so that
+# the backward sweep does not refactorise; False trades that memory for recomputation.
+RESIDUALS = True
 
 
 class GenerateFn(torch.autograd.Function):
@@ -78,14 +84,16 @@ class GenerateAndLogdetFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, xi, cov_vals, points, indices, neighbors, offsets, cov_bins, tau):
-        values, logdet = _gc.generate_and_logdet(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, tau=tau)
-        ctx.save_for_backward(xi, cov_vals, values)
+        out = _gc.generate_and_logdet(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, tau=tau,
+                                      with_resid=RESIDUALS)
+        values, logdet, resid = out if RESIDUALS else out + (None,)
+        ctx.save_for_backward(xi, cov_vals, values, resid)
         ctx.graph = (points, indices, neighbors, offsets, cov_bins, tau)
         return values, logdet
 
     @staticmethod
     def backward(ctx, g_values, g_logdet):
-        xi, cov_vals, values = ctx.saved_tensors
+        xi, cov_vals, values, resid = ctx.saved_tensors
         points, indices, neighbors, offsets, cov_bins, tau = ctx.graph
         need_xi, need_vals = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         if not (need_xi or need_vals):
@@ -94,7 +102,7 @@ class GenerateAndLogdetFn(torch.autograd.Function):
             g_values = torch.zeros_like(values)
         gl = 0.0 if g_logdet is None else float(g_logdet)
         gx, gv = _gc.generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi,
-                                  g_values.to(values.dtype).contiguous(), gl, tau=tau, values=values)
+                                  g_values.to(values.dtype).contiguous(), gl, tau=tau, values=values, resid=resid)
         return (gx if need_xi else None, gv.to(cov_vals.dtype) if need_vals else None) + (None,) * 6
 
 

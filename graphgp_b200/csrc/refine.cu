@@ -134,7 +134,7 @@ template <int D>
 cudaError_t dispatch_tpp(const RefineParams<float>& p, int kind, int nb, int max_blocks, cudaStream_t s, bool* done) {
   *done = false;
   const int k = p.k;
-  if (k > kTppMaxK || tpp_disabled()) return cudaSuccess;
+  if (k > kTppMaxK || tpp_disabled() || p.resid) return cudaSuccess;  // residuals: the four-lane kernel
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -466,10 +466,25 @@ int generate_impl(const T* points, const int32_t* perm, int64_t n, int d, int64_
 
 // generate and its log-determinant in one pass (FP32): the dense root writes sum log L_ii next to L xi, and the
 // refinement kernel (kOpGenerateLogdet) sums log std of every row into the per-block partials.
+// The adjoint's residuals come from the four-lane kernel (k <= 20, d in {2, 3}) when its shared memory fits the
+// table (checked for K = 20, the largest instantiation); elsewhere the adjoint recomputes them. For k up to
+// kTppMaxK the thread-per-point forward is kept: moving it to the four-lane kernel costs more than the adjoint's
+// refactorisation saves.
+bool resid_supported(int k, int d, int nb) {
+  if (k <= kTppMaxK || k > 20 || (d != 2 && d != 3)) return false;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t table = (table_smem_bytes<float>(nb) + 255) / 256 * 256;
+  const size_t per_warp = sizeof(float) * 8 * (d == 2 ? QuadSmem<20, 2>::kPerPoint : QuadSmem<20, 3>::kPerPoint);
+  return table + per_warp + kSmemHeadroom <= (size_t)optin;
+}
+
 int generate_and_logdet_f32_impl(const float* points, const int32_t* perm, int64_t n, int d, int64_t n0,
                                  const int32_t* nbrs, int k, const int32_t* offsets, int n_offsets, const float* bins,
                                  const float* vals, int nb, const float* xi, float* out, double* out_logdet,
-                                 double tau, uint64_t timeout_ns, void* wsp, size_t ws_bytes, cudaStream_t s) {
+                                 float* resid, int* resid_written, double tau, uint64_t timeout_ns, void* wsp,
+                                 size_t ws_bytes, cudaStream_t s) {
   using T = float;
   int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
@@ -489,6 +504,9 @@ int generate_and_logdet_f32_impl(const float* points, const int32_t* perm, int64
   p.perm = perm;
   p.out_user = out;
   p.gen_logdet = 1;
+  const bool with_resid = resid != nullptr && resid_supported(k, d, nb);
+  if (with_resid) p.resid = resid;
+  if (resid_written) *resid_written = with_resid ? 1 : 0;
   if (!perm) {
     p.perm = nullptr;
     p.out_user = nullptr;
@@ -643,11 +661,12 @@ int ggp_generate_f32(const float* points, const int32_t* indices, int64_t n, int
 int ggp_generate_and_logdet_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                                 const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                                 const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
-                                float* out_values, double* out_logdet, double tau, uint64_t timeout_ns,
-                                void* workspace, size_t workspace_bytes, ggp_stream_t stream) {
+                                float* out_values, double* out_logdet, float* out_resid, int* out_resid_written,
+                                double tau, uint64_t timeout_ns, void* workspace, size_t workspace_bytes,
+                                ggp_stream_t stream) {
   return generate_and_logdet_f32_impl(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
-                                      n_bins, xi, out_values, out_logdet, tau, timeout_ns, workspace, workspace_bytes,
-                                      GGP_STREAM(stream));
+                                      n_bins, xi, out_values, out_logdet, out_resid, out_resid_written, tau, timeout_ns,
+                                      workspace, workspace_bytes, GGP_STREAM(stream));
 }
 
 int ggp_generate_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
@@ -717,7 +736,7 @@ template <typename T>
 int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, int64_t n0, const int32_t* nbrs, int k,
                         const int32_t* offsets, int n_offsets, const T* bins, const T* vals, int nb, const T* xi,
                         const T* values, const T* g_values, double g_logdet, T* out_grad_xi, double* out_grad_vals,
-                        double tau, void* wsp, size_t ws_bytes, cudaStream_t s) {
+                        double tau, void* wsp, size_t ws_bytes, cudaStream_t s, const T* resid = nullptr) {
   int rc = check_refine_args(points, n, d, nbrs, k, offsets, n_offsets, bins, vals, nb, (int)sizeof(T));
   if (rc) return rc;
   if (n0 < 1 || n0 > n || !xi || !g_values || !out_grad_xi || !out_grad_vals) return GGP_ERR_INVALID;
@@ -757,6 +776,7 @@ int generate_vjp_device(const T* points, const int32_t* perm, int64_t n, int d, 
   v.hist_partials = partials;
   v.nb = nb;
   v.g_logdet = g_logdet;
+  v.resid = values ? resid : nullptr;  // residuals of this forward pass (generate's values given)
   bool swept = false;
   if (n > n0 && n_offsets > 1 && k <= 20 && (d == 2 || d == 3)) {
     cudaError_t e = d == 2 ? vjp_quad_dispatch_k<T, 2>(v, k, kVjpMaxGrid, s) : vjp_quad_dispatch_k<T, 3>(v, k, kVjpMaxGrid, s);
@@ -825,6 +845,17 @@ int ggp_generate_vjp_f32(const float* points, const int32_t* indices, int64_t n,
   return generate_vjp_device<float>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
                                     n_bins, xi, values, g_values, g_logdet, out_grad_xi, out_grad_vals, tau, workspace,
                                     workspace_bytes, GGP_STREAM(stream));
+}
+int ggp_generate_vjp_resid_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                               const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                               const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
+                               const float* values, const float* resid, const float* g_values, double g_logdet,
+                               float* out_grad_xi, double* out_grad_vals, double tau, void* workspace,
+                               size_t workspace_bytes, ggp_stream_t stream) {
+  if (!values || !resid) return GGP_ERR_INVALID;
+  return generate_vjp_device<float>(points, indices, n, d, n0, neighbors, k, offsets, n_offsets, cov_bins, cov_vals,
+                                    n_bins, xi, values, g_values, g_logdet, out_grad_xi, out_grad_vals, tau, workspace,
+                                    workspace_bytes, GGP_STREAM(stream), resid);
 }
 int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets, const double* cov_bins,

@@ -10,8 +10,9 @@ namespace ggp {
 enum RefineMode : int { kGenerate = 0, kInverse = 1 };
 
 // Compile-time operation of a refinement kernel instantiation.
-// kOpGenerateLogdet: generate that also sums log std of its rows into the log-determinant partials (FP32 only)
-enum RefineOp : int { kOpGenerate = 0, kOpInverse = 1, kOpLogdet = 2, kOpGenerateLogdet = 3 };
+// kOpGenerateLogdet: generate that also sums log std of its rows into the log-determinant partials (FP32 only);
+// kOpGenerateResid: the same, and it stores every row's adjoint residuals (RefineParams::resid; FP32, k <= 20)
+enum RefineOp : int { kOpGenerate = 0, kOpInverse = 1, kOpLogdet = 2, kOpGenerateLogdet = 3, kOpGenerateResid = 4 };
 
 template <typename T>
 struct RefineParams {
@@ -39,6 +40,8 @@ struct RefineParams {
                             // FP64 second pass instead of being re-conditioned in place; or null
   int table_smem;           // bytes of dynamic shared memory taken by the staged table (256-aligned)
   int gen_logdet;           // generate: also sum log std of every row into logdet_partials (one per block)
+  T* resid;                 // generate (FP32, k <= 20): per refined row w (k), a = K11^-1 v_N (k) and sigma, row
+                            // stride 2k + 1, for the adjoint; or null
   int sample_stride;        // FP32 inverse with a row list: > 0 runs the sampling pass over every sample_stride-th
                             // chunk (factor and count only); 0 is the ordinary pass
   unsigned long long timeout_ns;

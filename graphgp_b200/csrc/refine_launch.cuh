@@ -12,6 +12,8 @@ enum KernelKind { kCond = 0, kLogdet = 1 };
 // The generate-with-log-determinant operation exists for FP32 only (FP64 callers take two passes); for double this
 // names the plain generate instantiation, so no kernel is compiled twice.
 template <typename T> struct GenLogdetOp { static constexpr int value = sizeof(T) == 4 ? kOpGenerateLogdet : kOpGenerate; };
+// Generate with the adjoint's residuals: FP32 only (the host asks for it only there), likewise.
+template <typename T> struct GenResidOp { static constexpr int value = sizeof(T) == 4 ? kOpGenerateResid : kOpGenerate; };
 
 template <typename T, int K, int D, bool PAD>
 cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_blocks, cudaStream_t s);
@@ -37,8 +39,9 @@ cudaError_t launch_fast(const RefineParams<T>& p, int kind, int nb, int max_bloc
     const size_t smem = q.table_smem + per_warp * warps;
     auto kern = (kind != kCond) ? refine_quad2_kernel<T, K, D, PAD, kOpLogdet>
                 : (p.mode != kGenerate ? refine_quad2_kernel<T, K, D, PAD, kOpInverse>
-                   : (p.gen_logdet ? refine_quad2_kernel<T, K, D, PAD, GenLogdetOp<T>::value>
-                                   : refine_quad2_kernel<T, K, D, PAD, kOpGenerate>));
+                   : (p.resid ? refine_quad2_kernel<T, K, D, PAD, GenResidOp<T>::value>
+                      : (p.gen_logdet ? refine_quad2_kernel<T, K, D, PAD, GenLogdetOp<T>::value>
+                                      : refine_quad2_kernel<T, K, D, PAD, kOpGenerate>)));
     cudaError_t e = allow_smem(kern, smem);
     if (e != cudaSuccess) return e;
     if (max_blocks < 0) max_blocks = dataflow_blocks(p.n, p.n0, p.n_batches, block / 32);

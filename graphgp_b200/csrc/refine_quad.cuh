@@ -173,7 +173,7 @@ __device__ __forceinline__ void quad_load_coords(const RefineParams<T>& p, bool 
 template <typename T, int K>
 __device__ __forceinline__ T quad_mean(const RefineParams<T>& p, bool gen, bool may_wait,
                                        const int (&ids)[QuadRows<K>::NT], int g, const T (&wmine)[QuadRows<K>::NT],
-                                       bool& ok) {
+                                       bool& ok, T* vals_out = nullptr) {
   constexpr int NT = QuadRows<K>::NT;
   T val[NT];
 #pragma unroll
@@ -228,6 +228,10 @@ __device__ __forceinline__ T quad_mean(const RefineParams<T>& p, bool gen, bool 
   T part = T(0);
 #pragma unroll
   for (int t = 0; t < NT; ++t) part = fma(wmine[t], val[t], part);
+  if (vals_out) {
+#pragma unroll
+    for (int t = 0; t < NT; ++t) vals_out[t] = val[t];
+  }
   return quad_sum(part);
 }
 
@@ -472,9 +476,13 @@ __device__ __forceinline__ void quad_pairs(const T* __restrict__ crd, T* __restr
 // quad_factor with the off-diagonal covariances read from `tri` (pair (i, j), i > j, at i(i-1)/2 + j). Slot t of
 // this lane holds row i = 4t + g; for t > j / 4 every lane's row is below the diagonal of column j, so only
 // the slot holding the diagonal and the last slot (rows past K) need a per-lane test.
-template <typename T, int K>
+// With STORE_L the factor L11 is also left in shared memory for a later solve (quad_resid_a): its strictly lower
+// entries written over the pair array itself (entry (i, m) at i(i-1)/2 + m, the layout of the pairs it replaces,
+// once every pair has been read) and the reciprocal diagonal in rdiag[0..K).
+template <typename T, int K, bool STORE_L = false>
 __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g, int src0, T c0,
-                                                T (&wmine)[QuadRows<K>::NT], T& var, T& min_ratio) {
+                                                T (&wmine)[QuadRows<K>::NT], T& var, T& min_ratio,
+                                                T* __restrict__ rdiag = nullptr) {
   constexpr int R = K + 1;
   constexpr int NT = QuadRows<K>::NT;
   const T* trow[NT];  // pair row of this lane's row i: tri + i(i-1)/2
@@ -531,9 +539,59 @@ __device__ __forceinline__ void quad_factor_tri(const T* __restrict__ tri, int g
       }
     }
   }
+  if constexpr (STORE_L) {
+    __syncwarp();  // every lane has read its last pair entry
+#pragma unroll
+    for (int t = 0; t < QuadRows<K>::NT; ++t) {
+      const int i = t * kQuad + g;
+      if (i < K) {
+#pragma unroll
+        for (int m = 0; m < K; ++m)
+          if (m < i) const_cast<T*>(tri)[i * (i - 1) / 2 + m] = L[t][m];
+        rdiag[i] = L[t][i];  // 1 / L_ii
+      }
+    }
+  }
   quad_backsub<T, K>(L, g, src0, wmine);
   var = var_out;
   min_ratio = mr;
+}
+
+// a = K11^-1 v_N for the adjoint's residuals, from the factor quad_factor_tri<STORE_L> left in shared memory:
+// z = L11^-1 v_N by forward substitution (the owner of row i finishes z_i and broadcasts it; every lane updates its
+// rows below), then a = L11^-T z by backward substitution (quad sums, as in quad_backsub). val[t] holds the value
+// of this lane's row 4t + g (0 past K); amine[t] receives a of that row.
+template <typename T, int K>
+__device__ __forceinline__ void quad_resid_a(const T* __restrict__ lsm, const T* __restrict__ rdiag,
+                                             const T (&val)[QuadRows<K>::NT], int g, int src0,
+                                             T (&amine)[QuadRows<K>::NT]) {
+  constexpr int NT = QuadRows<K>::NT;
+  T z[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) z[t] = val[t];
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const T zi = __shfl_sync(0xffffffffu, z[i / kQuad] * rdiag[i], src0 + i % kQuad);
+    if (g == i % kQuad) z[i / kQuad] = zi;
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int r = t * kQuad + g;
+      if (t * kQuad + kQuad - 1 > i && r > i && r < K) z[t] = fma(-lsm[r * (r - 1) / 2 + i], zi, z[t]);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < NT; ++t) amine[t] = T(0);
+#pragma unroll
+  for (int m = K - 1; m >= 0; --m) {
+    T part = T(0);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int r = t * kQuad + g;
+      if (t * kQuad + kQuad - 1 > m && r > m && r < K) part = fma(lsm[r * (r - 1) / 2 + m], amine[t], part);
+    }
+    part = quad_sum(part);
+    if (g == m % kQuad) amine[m / kQuad] = (z[m / kQuad] - part) * rdiag[m];
+  }
 }
 
 // MODE is the operation, fixed at compile time (kOpGenerate, kOpInverse, kOpLogdet): the generate kernel carries no
@@ -560,8 +618,9 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
   const int src0 = lane & ~(kQuad - 1);
   T* crd = scratch + q * SM::kPerPoint;                      // (K+1) x kPointStride
   T* tri = crd + (K + 1) * SM::kPointStride;                 // kPairs
-  constexpr bool gen = MODE == kOpGenerate || MODE == kOpGenerateLogdet;
-  constexpr bool GENLD = MODE == kOpGenerateLogdet;
+  constexpr bool RESID = MODE == kOpGenerateResid;
+  constexpr bool gen = MODE == kOpGenerate || MODE == kOpGenerateLogdet || RESID;
+  constexpr bool GENLD = MODE == kOpGenerateLogdet || RESID;
   const unsigned int total = (unsigned int)__ldg(p.chunk_prefix + p.n_batches);
   const bool may_wait = ld_relaxed(reinterpret_cast<const int*>(&p.status->error)) == 0;
   double acc_logdet = 0.0;
@@ -600,7 +659,7 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
       quad_pairs<T, K, D, PAD>(crd, tri, g, p.k, tab);
       __syncwarp();
       T wmine[NT], var, mr;
-      quad_factor_tri<T, K>(tri, g, src0, c0, wmine, var, mr);
+      quad_factor_tri<T, K, RESID>(tri, g, src0, c0, wmine, var, mr, crd);  // RESID: L11 stays in tri / crd
       __syncwarp();  // the scratch is reused by the next sub-iteration
       mr = quad_min(mr);
       const bool fb = sizeof(T) == 4 && active && !(mr >= (T)p.tau);  // quad-uniform
@@ -611,7 +670,8 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
       if (fb && !defer && g == 0) quad_refactor_f64<T, K, D>(p, row, w64, vd64);
       // every lane runs quad_mean (its quad sum is a full-warp shuffle), deferred points included
       T mean = T(0);
-      if (!LOGDET) mean = quad_mean<T, K>(p, gen, may_wait, ids, g, wmine, ok);
+      T vals[NT];
+      if (!LOGDET) mean = quad_mean<T, K>(p, gen, may_wait, ids, g, wmine, ok, RESID ? vals : nullptr);
       int okv = ok ? 1 : 0;  // quad-wide AND, both shuffles executed by every lane
       okv &= __shfl_xor_sync(0xffffffffu, okv, 1);
       okv &= __shfl_xor_sync(0xffffffffu, okv, 2);
@@ -619,6 +679,25 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
         if (sampling) sample_row(p, fb);
         else if (defer) list_row(p, row);  // constant false in the generate instantiation
         else quad_finish<T, K, D, LOGDET, GENLD>(p, gen, row, okv != 0, mean, var, fb, w64, vd64, acc_logdet);
+      }
+      if constexpr (RESID) {  // the adjoint's residuals: w, a = K11^-1 v_N and sigma of this row, once
+                              // the value is published (off the dependency chain)
+        T amine[NT];
+        quad_resid_a<T, K>(tri, crd, vals, g, src0, amine);
+        if (active) {
+          const int kk = p.k;
+          T* rr = p.resid + (row - p.n0) * (2 * kk + 1);
+#pragma unroll
+          for (int tt = 0; tt < NT; ++tt) {
+            const int i = tt * kQuad + g;
+            if (i < kk) {
+              rr[i] = wmine[tt];
+              rr[kk + i] = amine[tt];
+            }
+          }
+          if (g == 0) rr[2 * kk] = sqrt(var);
+        }
+        __syncwarp();  // L11 in the scratch is read to the end before the next sub-iteration overwrites it
       }
     }
   }

@@ -17,6 +17,7 @@ struct VjpParams {
   double* hist_partials;        // (gridDim.x, nb)
   int nb;
   double g_logdet;
+  const T* resid;               // the forward's residuals (w, a, sigma per refined row, stride 2k + 1), or null
 };
 
 // Bracket and weight of radius r: cov_lookup(r) = (1 - t) vals[j] + t vals[j + 1].

@@ -6,7 +6,7 @@
 //  1. before any wait: the pair covariances into shared memory, a left-looking Cholesky of the rows
 //     [nbr_0 .. nbr_{k-1}, self, v] (v = the neighbours' forward values, so that row becomes z = L11^-1 v),
 //     and a two-right-hand-side back substitution giving w = L11^-T l21 and a = L11^-T z in the lanes that
-//     own the rows;
+//     own the rows; or, when the forward pass kept them (VjpParams::resid), w, a and sigma read back;
 //  2. wait until every row of the later batches has finished (a row-granular completion count; those rows
 //     hold earlier tickets, so the bounded wait always ends), read the final cotangent vbar_i, write
 //     xibar_i = sigma_i vbar_i and scatter w_m vbar_i into the neighbours' cotangents, then count the rows
@@ -155,12 +155,6 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
       int ids[NT];
       T P[NT][D];
       quad_load_coords<T, K, D, PAD>(p, active, true, active ? row : bstart, bstart, g, ids, P, ok);
-      T val[NT];
-#pragma unroll
-      for (int t = 0; t < NT; ++t) {
-        const int i = t * kQuad + g;
-        val[t] = (i < K && ids[t] >= 0) ? __ldg(p.values + ids[t]) : T(0);
-      }
 #pragma unroll
       for (int tt = 0; tt < NT; ++tt) {
         const int i = tt * kQuad + g;
@@ -169,13 +163,33 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
           for (int c = 0; c < D; ++c) crd[i * SM::kPointStride + c] = P[tt][c];
         }
       }
-      __syncwarp();
-      quad_pairs<T, K, D, PAD>(crd, tri, g, kk, tab);  // pair covariances, dealt p = g, g+4, ...
-      __syncwarp();
-      T wmine[NT], amine[NT], var;
-      quad_factor_wa<T, K, NT>(tri, val, g, src0, c0, wmine, amine, var);
-      const T sig = sqrt(var);
-      __syncwarp();  // tri is reused for w and a below
+      T wmine[NT], amine[NT], sig;
+      if (v.resid) {  // warp-uniform: w, a and sigma as the forward pass left them
+        const T* rr = v.resid + (active ? row - p.n0 : 0) * (2 * kk + 1);
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+          const int i = t * kQuad + g;
+          const bool in = active && i < K && (!PAD || i < kk);
+          wmine[t] = in ? __ldg(rr + i) : T(0);
+          amine[t] = in ? __ldg(rr + kk + i) : T(0);
+        }
+        sig = active ? __ldg(rr + 2 * kk) : T(1);
+        __syncwarp();  // the coordinates are read by other lanes of the quad below
+      } else {
+        T val[NT];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+          const int i = t * kQuad + g;
+          val[t] = (i < K && ids[t] >= 0) ? __ldg(p.values + ids[t]) : T(0);
+        }
+        __syncwarp();
+        quad_pairs<T, K, D, PAD>(crd, tri, g, kk, tab);  // pair covariances, dealt p = g, g+4, ...
+        __syncwarp();
+        T var;
+        quad_factor_wa<T, K, NT>(tri, val, g, src0, c0, wmine, amine, var);
+        sig = sqrt(var);
+        __syncwarp();  // tri is reused for w and a below
+      }
       // wait for the later batches (lane 0 for the warp)
       if (lane == 0 && !waited_out) {
         const uint64_t t_start = global_timer_ns();

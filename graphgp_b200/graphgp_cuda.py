@@ -347,12 +347,17 @@ def generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau
     return out
 
 
-def generate_and_logdet(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau=None, timeout_ns=0):
+def generate_and_logdet(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, *, tau=None, timeout_ns=0,
+                        with_resid=False):
     """``generate`` and ``generate_logdet`` of the same table -> (values (N,), logdet (0-d float64)). In FP32 one
-    pass computes both (``ggp_generate_and_logdet_f32``); in FP64 the two calls run one after the other."""
+    pass computes both (``ggp_generate_and_logdet_f32``); in FP64 the two calls run one after the other.
+
+    ``with_resid``: also return the adjoint's residuals ((N - n0) x (2k + 1) FP32, for ``generate_vjp(resid=...)``)
+    as a third element, or None where the pass does not write them (FP64, k > 20, d not in {2, 3})."""
     if _suffix(_cuda(points, "points").dtype) != "f32":
-        return (generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, tau=tau, timeout_ns=timeout_ns),
-                generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, tau=tau))
+        out = (generate(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, tau=tau, timeout_ns=timeout_ns),
+               generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, tau=tau))
+        return out + (None,) if with_resid else out
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
     xi = _cuda(xi, "xi", points.dtype)
@@ -362,11 +367,18 @@ def generate_and_logdet(points, indices, neighbors, offsets, cov_bins, cov_vals,
     out = torch.empty(n, dtype=points.dtype, device=points.device)
     ld = torch.empty((), dtype=torch.float64, device=points.device)
     ws = _workspace("GENERATE", n, d, n0, k, len(bins), len(offs), points.element_size(), points.device)
+    resid = None
+    written = C.c_int(0)
+    if with_resid and n > n0 and k <= 20 and d in (2, 3):
+        resid = torch.empty((n - n0, 2 * k + 1), dtype=torch.float32, device=points.device)
     rc = _lib.load().ggp_generate_and_logdet_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
                                                  _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(out), _ptr(ld),
-                                                 _tau(tau), int(timeout_ns), _ptr(ws), ws.numel(), _stream())
+                                                 _ptr(resid), C.byref(written), _tau(tau), int(timeout_ns),
+                                                 _ptr(ws), ws.numel(), _stream())
     _lib.check(rc, "generate_and_logdet")
-    return out, ld
+    if not with_resid:
+        return out, ld
+    return out, ld, (resid if written.value else None)
 
 
 def generate_inv(points, indices, neighbors, offsets, cov_bins, cov_vals, values, *, tau=None):
@@ -410,11 +422,13 @@ def generate_logdet(points, neighbors, offsets, cov_bins, cov_vals, *, tau=None)
 
 
 def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_values, g_logdet=0.0, *,
-                 tau=None, values=None):
+                 tau=None, values=None, resid=None):
     """Adjoint of generate (+ g_logdet * generate_logdet): returns (grad_xi (N,), grad_cov_vals (n_bins,) f64).
 
     ``values``: generate's output for these same inputs, if the caller has it (the primal output a custom_vjp
-    keeps); it saves recomputing the forward pass. Per-point factorisations are recomputed either way."""
+    keeps); it saves recomputing the forward pass. ``resid``: the residuals ``generate_and_logdet(with_resid=True)``
+    returned for the same inputs (FP32, needs ``values``); the reverse sweep then reads each row's w, a and sigma
+    instead of refactorising it. Without them the per-point factorisations are recomputed."""
     points, sfx, nb, n, d, n0, k, offs = _refine_common(points, neighbors, offsets)
     bins, vals = _table(cov_bins, cov_vals, points.dtype)
     xi = _cuda(xi, "xi", points.dtype)
@@ -430,7 +444,17 @@ def generate_vjp(points, indices, neighbors, offsets, cov_bins, cov_vals, xi, g_
     gv = torch.empty(len(bins), dtype=torch.float64, device=points.device)
     ws = _workspace("GENERATE_VJP", n, d, n0, k, len(bins), len(offs), points.element_size(), points.device)
     lib = _lib.load()
-    if sfx == "f32":
+    if resid is not None:
+        if sfx != "f32" or values is None:
+            raise ValueError("resid needs FP32 inputs and values")
+        resid = _cuda(resid, "resid", torch.float32)
+        if resid.numel() != (n - n0) * (2 * k + 1):
+            raise ValueError("resid must hold (N - n0) x (2k + 1) entries")
+        rc = lib.ggp_generate_vjp_resid_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
+                                            _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(values), _ptr(resid),
+                                            _ptr(g), float(g_logdet), _ptr(gx), _ptr(gv), _tau(tau), _ptr(ws),
+                                            ws.numel(), _stream())
+    elif sfx == "f32":
         rc = lib.ggp_generate_vjp_f32(_ptr(points), _ptr(idx), n, d, n0, _ptr(nb), k, _ptr(offs), len(offs),
                                       _ptr(bins), _ptr(vals), len(bins), _ptr(xi), _ptr(values), _ptr(g),
                                       float(g_logdet), _ptr(gx),

@@ -238,11 +238,16 @@ int ggp_generate_f64(const double* points, const int32_t* indices, int64_t n, in
 /* generate and generate_logdet of the same table in one pass (FP32; no counterpart in the reference, where a    */
 /* loss using both calls each): values as ggp_generate_f32, and the log-determinant (as ggp_generate_logdet_f32, */
 /* device FP64) summed from the same factorisations. Workspace: ggp_workspace_size(GGP_OP_GENERATE, ...).       */
+/* out_resid (optional, (n - n0) x (2k + 1) floats, refined rows in graph order): the adjoint's residuals of    */
+/* each refined row, w = K11^-1 k12 (k), a = K11^-1 v_N (k, v_N the neighbours' values) and sigma, for          */
+/* ggp_generate_vjp_resid_f32. They are written only where the four-lane kernel runs (k <= 20, d in {2, 3},     */
+/* the table in shared memory); *out_resid_written (optional) is set to 1 when they were, else 0.               */
 int ggp_generate_and_logdet_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                                 const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                                 const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
-                                float* out_values, double* out_logdet, double tau, uint64_t timeout_ns,
-                                void* workspace, size_t workspace_bytes, ggp_stream_t stream);
+                                float* out_values, double* out_logdet, float* out_resid, int* out_resid_written,
+                                double tau, uint64_t timeout_ns, void* workspace, size_t workspace_bytes,
+                                ggp_stream_t stream);
 int ggp_generate_inv_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                          const float* cov_bins, const float* cov_vals, int n_bins, const float* values,
@@ -267,7 +272,8 @@ int ggp_generate_logdet_f64(const double* points, int64_t n, int d, int64_t n0, 
 /* scalar cotangent g_logdet for generate_logdet, writes                                            */
 /*   out_grad_xi (n,)        = d/dxi  <g_values, generate(xi)>                                       */
 /*   out_grad_vals (n_bins,) = d/dcov_vals [<g_values, generate(xi)> + g_logdet * generate_logdet]   */
-/* out_grad_vals is FP64. Per-point Cholesky factors are recomputed, never stored. `values` is       */
+/* out_grad_vals is FP64. Per-point Cholesky factors are recomputed (ggp_generate_vjp_resid_f32: read  */
+/* from the forward's residuals instead). `values` is                                               */
 /* generate's output for the same inputs (caller order), the primal output a custom_vjp keeps as its  */
 /* residual: passing it skips recomputing the forward pass; NULL recomputes it.                     */
 /* ---------------------------------------------------------------------------------------------- */
@@ -277,6 +283,14 @@ int ggp_generate_vjp_f32(const float* points, const int32_t* indices, int64_t n,
                          const float* values, const float* g_values, double g_logdet, float* out_grad_xi,
                          double* out_grad_vals, double tau, void* workspace, size_t workspace_bytes,
                          ggp_stream_t stream);
+/* As ggp_generate_vjp_f32 with the residuals ggp_generate_and_logdet_f32 wrote for the same inputs (`values`  */
+/* and `resid` both required): the four-lane reverse sweep reads w, a and sigma instead of refactorising.       */
+int ggp_generate_vjp_resid_f32(const float* points, const int32_t* indices, int64_t n, int d, int64_t n0,
+                               const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
+                               const float* cov_bins, const float* cov_vals, int n_bins, const float* xi,
+                               const float* values, const float* resid, const float* g_values, double g_logdet,
+                               float* out_grad_xi, double* out_grad_vals, double tau, void* workspace,
+                               size_t workspace_bytes, ggp_stream_t stream);
 int ggp_generate_vjp_f64(const double* points, const int32_t* indices, int64_t n, int d, int64_t n0,
                          const int32_t* neighbors, int k, const int32_t* offsets, int n_offsets,
                          const double* cov_bins, const double* cov_vals, int n_bins, const double* xi,

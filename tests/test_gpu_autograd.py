@@ -77,3 +77,33 @@ def test_backward_equals_adjoint_fp32(cuda_device):
     np.testing.assert_allclose(xi.grad.cpu().numpy(), gx.cpu().numpy(), rtol=1e-5, atol=1e-5 * float(gx.abs().max()))
     np.testing.assert_allclose(vals.grad.double().cpu().numpy(), gv.float().double().cpu().numpy(), rtol=1e-5,
                                atol=1e-5 * float(gv.abs().max()))
+
+
+@pytest.mark.parametrize("k,d", [(16, 2), (20, 3), (13, 3), (7, 2)])
+def test_backward_with_and_without_residuals(cuda_device, k, d):
+    """GenerateAndLogdetFn's backward reading the forward's residuals equals the refactorising backward (FP32
+    rounding: a = K11^-1 v_N is solved in another order)."""
+    import torch
+
+    import graphgp_b200 as gg
+    from graphgp_b200 import autograd as ag
+
+    graph, B, V = _graph(cuda_device, torch.float32, n=4000, d=d, n0=100, k=k)
+    n = len(graph.points)
+    gen = torch.Generator(device=cuda_device).manual_seed(k)
+    y = torch.randn(n, generator=gen, device=cuda_device)
+    xi0 = torch.randn(n, generator=gen, device=cuda_device)
+    grads = []
+    saved = ag.RESIDUALS
+    try:
+        for flag in (True, False):
+            ag.RESIDUALS = flag
+            xi = xi0.clone().requires_grad_(True)
+            vals = V.clone().requires_grad_(True)
+            v, ld = gg.generate_and_logdet(graph, (B, vals), xi)
+            (0.5 * torch.sum((v - y) ** 2) + ld).backward()
+            grads.append((xi.grad.cpu().numpy(), vals.grad.double().cpu().numpy()))
+    finally:
+        ag.RESIDUALS = saved
+    for a, b in zip(grads[0], grads[1]):
+        np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-5 * float(np.abs(b).max()))

@@ -175,3 +175,63 @@ def test_vjp_with_forward_values_matches_recompute(cuda_device, n, d, n0, k, tab
         b_x, b_v = gc.generate_vjp(*args, _t(gv, cuda_device, dt), gl, values=v)
         assert rel_err(b_x.cpu().numpy(), a_x.cpu().numpy()) < tol, dt
         assert rel_err(b_v.cpu().numpy(), a_v.cpu().numpy()) < tol, dt
+
+
+# k above the thread-per-point range (10) and up to 20, d in {2, 3}: the forward keeps residuals (13 and 18 pad to
+# the 16- and 20-slot kernels)
+RESID_CASES = [(2500, 3, 128, 16, "matern", 0.7), (1500, 2, 64, 20, "rbf", -1.3), (1800, 3, 100, 13, "matern", 0.0),
+               (2200, 2, 300, 18, "rbf", 0.4)]
+
+
+@pytest.mark.parametrize("n,d,n0,k,tab,gl", RESID_CASES)
+@pytest.mark.parametrize("with_indices", [True, False])
+def test_vjp_with_forward_residuals(cuda_device, n, d, n0, k, tab, gl, with_indices):
+    """The one-pass forward's residuals (w, a, sigma per refined row) give the gradients of the refactorising
+    adjoint: to 1e-5 (FP32; a = K11^-1 v_N is solved in another order) and to the oracle's tolerances."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    pts, g = oracle_graph(n, d, n0, k)
+    bins, vals = as_inputs(_table(tab), np.float32)
+    rng = np.random.default_rng(n + 23)
+    xi, gv = rng.standard_normal(n), rng.standard_normal(n)
+    rx, rv = oa.generate_vjp(g, (bins, vals), xi, gv, gl)
+    f32 = torch.float32
+    idx = _t(g.indices, cuda_device) if with_indices else None
+    # without indices every per-point array is in graph order: row r holds original point indices[r]
+    xi_t = _t(xi if with_indices else xi[g.indices], cuda_device, f32)
+    gv_t = _t(gv if with_indices else gv[g.indices], cuda_device, f32)
+    pts_t = _t(g.points, cuda_device, f32)
+    args = (pts_t, idx, _t(g.neighbors, cuda_device), g.offsets, _t(bins, cuda_device, f32),
+            _t(vals, cuda_device, f32), xi_t)
+    v, ld, resid = gc.generate_and_logdet(*args, with_resid=True)
+    assert resid is not None and tuple(resid.shape) == (n - n0, 2 * k + 1)
+    assert bool(torch.isfinite(resid).all()) and bool((resid[:, 2 * k] > 0).all())
+    a_x, a_v = gc.generate_vjp(*args, gv_t, gl, values=v)
+    b_x, b_v = gc.generate_vjp(*args, gv_t, gl, values=v, resid=resid)
+    st = gc.last_status()
+    assert st["error"] == 0 and st["timeouts"] == 0
+    assert rel_err(b_x.cpu().numpy(), a_x.cpu().numpy()) < 1e-5
+    assert rel_err(b_v.cpu().numpy(), a_v.cpu().numpy()) < 1e-5
+    assert rel_err(b_x.cpu().numpy(), rx if with_indices else rx[g.indices]) < 1e-4
+    assert rel_err(b_v.cpu().numpy(), rv) < 1e-3
+
+
+@pytest.mark.parametrize("k", [32, 10])
+def test_residuals_absent_outside_four_lane_kernel(cuda_device, k):
+    """k = 32 has no four-lane kernel and k = 10 keeps the thread-per-point forward: no residuals (None), and the
+    values are those of the call without them."""
+    import torch
+    from graphgp_b200 import graphgp_cuda as gc
+
+    n, d, n0 = 1500, 2, 64
+    pts, g = oracle_graph(n, d, n0, k)
+    bins, vals = as_inputs(rbf_table(scale=0.3), np.float32)
+    f32 = torch.float32
+    xi = np.random.default_rng(3).standard_normal(n)
+    args = (_t(g.points, cuda_device, f32), _t(g.indices, cuda_device), _t(g.neighbors, cuda_device), g.offsets,
+            _t(bins, cuda_device, f32), _t(vals, cuda_device, f32), _t(xi, cuda_device, f32))
+    v, ld, resid = gc.generate_and_logdet(*args, with_resid=True)
+    assert resid is None
+    v2, ld2 = gc.generate_and_logdet(*args)
+    assert torch.equal(v, v2)
