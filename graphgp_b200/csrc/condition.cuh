@@ -34,11 +34,13 @@ __device__ __forceinline__ T point_distance(const T (&a)[D], const T (&b)[D]) {
 // budget. Row-oriented (Cholesky-Banachiewicz) factorisation of the order-(k+1) joint matrix, then back
 // substitution L11^T w = l21. Only coordinates and the table are read: no neighbour value is needed, so a
 // point computes this before it waits for its neighbours. `ids` are the neighbour ids, `self` the point's
-// own row.
+// own row. With `values` and `a` (the adjoint's use) also a = K11^-1 v_N for the neighbours' values v_N:
+// z = L11^-1 v_N by forward substitution, then a = L11^-T z in place.
 template <typename TP, int KM>
 __device__ __noinline__ void condition_weights_f64(const TP* __restrict__ points, int d, long long self,
                                                    const int* ids, int k, const TableView<double> tab, double c0,
-                                                   double* w, double* out_var) {
+                                                   double* w, double* out_var, const TP* values = nullptr,
+                                                   double* a = nullptr) {
   double A[(KM + 1) * (KM + 2) / 2];
   const int n = k + 1;
 #pragma unroll 1
@@ -80,6 +82,21 @@ __device__ __noinline__ void condition_weights_f64(const TP* __restrict__ points
     w[m] = s / A[m * (m + 1) / 2 + m];
   }
   *out_var = rk[k];
+  if (a) {
+#pragma unroll 1
+    for (int i = 0; i < k; ++i) {
+      const double* ri = A + i * (i + 1) / 2;
+      double s = (double)values[ids[i]];
+      for (int m = 0; m < i; ++m) s = fma(-ri[m], a[m], s);
+      a[i] = s / ri[i];
+    }
+#pragma unroll 1
+    for (int m = k - 1; m >= 0; --m) {
+      double s = a[m];
+      for (int i = m + 1; i < k; ++i) s = fma(-A[i * (i + 1) / 2 + m], a[i], s);
+      a[m] = s / A[m * (m + 1) / 2 + m];
+    }
+  }
 }
 
 }  // namespace ggp

@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(Quad2Block<T>::kMax, 1) refine_quad2_kernel(Re
               rr[kk + i] = amine[tt];
             }
           }
-          if (g == 0) rr[2 * kk] = sqrt(var);
+          if (g == 0) rr[2 * kk] = fb ? T(-1) : sqrt(var);  // -1: re-conditioned in FP64, the adjoint redoes it
         }
         __syncwarp();  // L11 in the scratch is read to the end before the next sub-iteration overwrites it
       }

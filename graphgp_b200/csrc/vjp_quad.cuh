@@ -55,10 +55,11 @@ __device__ __forceinline__ void quad_backsub_wa(const T (&L)[NT][K + 1], int g, 
 }
 
 // Left-looking Cholesky of [nbrs, self, v] from the pair covariances in `tri` and the values `val` of this
-// lane's rows, then w and a. Returns var = sigma^2 in every lane.
+// lane's rows, then w and a. Returns var = sigma^2 and the smallest pivot over c0 (the forward's
+// re-conditioning test) in every lane.
 template <typename T, int K, int NT>
 __device__ __forceinline__ void quad_factor_wa(const T* __restrict__ tri, const T (&val)[NT], int g, int src0, T c0,
-                                               T (&wmine)[NT], T (&amine)[NT], T& var) {
+                                               T (&wmine)[NT], T (&amine)[NT], T& var, T& min_ratio) {
   constexpr int R = K + 2;  // rows: K neighbours, self, v
   T L[NT][K + 1];
 #pragma unroll
@@ -66,6 +67,8 @@ __device__ __forceinline__ void quad_factor_wa(const T* __restrict__ tri, const 
 #pragma unroll
     for (int m = 0; m <= K; ++m) L[t][m] = T(0);
   T var_out = T(0);
+  T mr = T(1);
+  const T inv_c0 = T(1) / c0;
 #pragma unroll
   for (int j = 0; j <= K; ++j) {
     const int tj = j / kQuad;
@@ -92,6 +95,7 @@ __device__ __forceinline__ void quad_factor_wa(const T* __restrict__ tri, const 
         if (t * kQuad + kQuad - 1 >= j) acc[t] = fma(-L[t][m], b, acc[t]);
     }
     const T s = __shfl_sync(0xffffffffu, acc[tj], src);
+    mr = fmin(mr, s * inv_c0);
     if (j == K) var_out = s;
     const T r = fast_rsqrt<T>(s);
 #pragma unroll
@@ -102,6 +106,22 @@ __device__ __forceinline__ void quad_factor_wa(const T* __restrict__ tri, const 
   }
   quad_backsub_wa<T, K, NT>(L, g, src0, wmine, amine);
   var = var_out;
+  min_ratio = mr;
+}
+
+// FP64 w, a and sigma^2 of one row (lane 0 of its quad), for the rows the FP32 forward re-conditions in FP64
+// (smallest pivot ratio below tau): the adjoint of the forward as it ran. Neighbour values from p.values.
+template <typename T, int K, int D>
+__device__ __forceinline__ void quad_refactor_wa_f64(const RefineParams<T>& p, long long row, double (&w64)[K],
+                                                     double (&a64)[K], double& vd64) {
+  const long long r0 = row - p.n0;
+  int ids[K];
+  for (int m = 0; m < p.k && m < K; ++m) {
+    const int id = __ldg(p.nbrs + r0 * p.k + m);
+    ids[m] = (id < 0 || (long long)id >= p.n) ? 0 : id;
+  }
+  condition_weights_f64<T, K>(p.points, D, row, ids, p.k, global_table_view<double>(p.tb), p.tb.desc->c0, w64, &vd64,
+                              p.values, a64);
 }
 
 template <typename T, int K, int D, bool PAD, int BLOCK>
@@ -109,7 +129,7 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
   const RefineParams<T>& p = v.r;
   constexpr int NT = (K + 2 + kQuad - 1) / kQuad;
   using SM = QuadSmem<K, D>;
-  static_assert(2 * K <= SM::kPairs, "w and a reuse the pair scratch");
+  static_assert(2 * K + 1 <= SM::kPairs, "w, a and sigma reuse the pair scratch");
   static_assert(NT == QuadRows<K>::NT, "the v row must fit in the slots of the point rows");
   extern __shared__ __align__(32) unsigned char smem[];
   const TableView<T> tab = stage_table<T>(p.tb, smem);
@@ -164,6 +184,7 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
         }
       }
       T wmine[NT], amine[NT], sig;
+      bool fb = false;  // quad-uniform: the row the FP32 forward re-conditioned in FP64
       if (v.resid) {  // warp-uniform: w, a and sigma as the forward pass left them
         const T* rr = v.resid + (active ? row - p.n0 : 0) * (2 * kk + 1);
 #pragma unroll
@@ -174,6 +195,7 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
           amine[t] = in ? __ldg(rr + kk + i) : T(0);
         }
         sig = active ? __ldg(rr + 2 * kk) : T(1);
+        fb = sizeof(T) == 4 && active && !(sig > T(0));  // the forward marks its re-conditioned rows with -1
         __syncwarp();  // the coordinates are read by other lanes of the quad below
       } else {
         T val[NT];
@@ -185,10 +207,36 @@ __global__ void __launch_bounds__(BLOCK) vjp_quad_kernel(VjpParams<T> v) {
         __syncwarp();
         quad_pairs<T, K, D, PAD>(crd, tri, g, kk, tab);  // pair covariances, dealt p = g, g+4, ...
         __syncwarp();
-        T var;
-        quad_factor_wa<T, K, NT>(tri, val, g, src0, c0, wmine, amine, var);
+        T var, mr;
+        quad_factor_wa<T, K, NT>(tri, val, g, src0, c0, wmine, amine, var, mr);
         sig = sqrt(var);
+        const T mq = quad_min(mr);  // every lane executes the shuffles (no short-circuit around a warp intrinsic)
+        fb = sizeof(T) == 4 && active && !(mq >= (T)p.tau);
         __syncwarp();  // tri is reused for w and a below
+      }
+      if constexpr (sizeof(T) == 4) {
+        // as the forward: a row whose FP32 pivots fell below tau takes w, a and sigma from an FP64 factorisation
+        if (fb && g == 0) {
+          double w64[K], a64[K], vd64;
+          quad_refactor_wa_f64<T, K, D>(p, row, w64, a64, vd64);
+          for (int i = 0; i < K; ++i) {
+            tri[i] = i < kk ? (T)w64[i] : T(0);
+            tri[K + i] = i < kk ? (T)a64[i] : T(0);
+          }
+          tri[2 * K] = (T)sqrt(vd64);
+          atomicAdd(&p.status->fallback_count, 1u);
+        }
+        __syncwarp();
+        if (fb) {
+#pragma unroll
+          for (int t = 0; t < NT; ++t) {
+            const int i = t * kQuad + g;
+            wmine[t] = i < K ? tri[i] : T(0);
+            amine[t] = i < K ? tri[K + i] : T(0);
+          }
+          sig = tri[2 * K];
+        }
+        __syncwarp();
       }
       // wait for the later batches (lane 0 for the warp)
       if (lane == 0 && !waited_out) {
