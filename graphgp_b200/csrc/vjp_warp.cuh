@@ -7,7 +7,8 @@
 // it factors each of the chunk's points: the covariances of [nbrs, self] from the table, a right-looking Cholesky
 // of [nbrs, self, v] (the neighbour values as a last row, so that the factorisation leaves z = L11^-1 v_N there),
 // sigma = L[k][k], and w = L11^-T l21, a = L11^-T z by backward substitution with lane m holding entry m. The
-// chunk's w, a, sigma and ids wait in a per-warp buffer (coordinates are gathered again after the wait). The wait:
+// chunk's w, a, sigma and ids wait in a per-warp buffer (coordinates are gathered again after the wait); in FP32 a
+// point whose pivots fell below tau takes them from an FP64 factorisation instead, as in the forward. The wait:
 // every chunk of the later batches finished (a chunk-granular completion counter; those chunks hold earlier
 // tickets). On the chain: xibar = sigma vbar and the scatter of w_m vbar into the neighbours' cotangents, then the
 // chunk is counted. Off the chain: the derivatives of (mean, sigma) with respect to every covariance entry into
@@ -127,6 +128,31 @@ __device__ __forceinline__ void vjp_warp_factor(const RefineParams<T>& p, const 
   if (lane < k) {
     S.W[pt * k + lane] = ws;
     S.Aa[pt * k + lane] = as;
+  }
+  if constexpr (sizeof(T) == 4) {
+    // as the forward: a point whose FP32 pivots fell below tau (smallest L_jj^2 / c0, a NaN pivot counted as
+    // -1) takes w, a and sigma from one FP64 factorisation
+    T mr = T(1);
+    for (int j = lane; j <= k; j += 32) {
+      const T djj = S.A[vw_packed(j, j)];
+      T r = djj * djj / c0;
+      if (!(r == r)) r = T(-1);
+      mr = fmin(mr, r);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mr = fmin(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    __syncwarp();  // every lane's w and a are stored before lane 0 may overwrite them
+    if (!(mr >= (T)p.tau) && lane == 0) {  // the test is warp-uniform
+      double w64[kVjpMaxK], a64[kVjpMaxK], vd64;
+      condition_weights_f64<T, kVjpMaxK>(p.points, d, row, ids, k, global_table_view<double>(p.tb), p.tb.desc->c0,
+                                         w64, &vd64, p.values, a64);
+      for (int m = 0; m < k; ++m) {
+        S.W[pt * k + m] = (T)w64[m];
+        S.Aa[pt * k + m] = (T)a64[m];
+      }
+      S.sig[pt] = (T)sqrt(vd64);
+      atomicAdd(&p.status->fallback_count, 1u);
+    }
   }
   __syncwarp();  // the matrix is reused by the next point
 }

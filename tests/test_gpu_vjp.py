@@ -237,11 +237,12 @@ def test_residuals_absent_outside_four_lane_kernel(cuda_device, k):
     assert torch.equal(v, v2)
 
 
-@pytest.mark.parametrize("k", [16, 10])
+@pytest.mark.parametrize("k", [16, 10, 24, 32])
 def test_vjp_f32_reconditioned_rows(cuda_device, k):
     """Near-duplicate points (a 2-d shell of radii 10^U(-3, 0)) push some FP32 pivots below tau. The forward
     re-conditions those rows in FP64, and so does the adjoint: w, a and sigma from one FP64 factorisation (the
-    residual-reading sweep too, where the forward marks the rows). The FP32 gradients stay finite and follow the
+    four-lane sweep for k <= 20, the warp-per-point sweep for 24 and 32, and the residual-reading sweep, where
+    the forward marks the rows). The FP32 gradients stay finite and follow the
     FP64 adjoint; the two FP32 sweeps agree to 1e-5."""
     import torch
     from graphgp_b200 import graphgp_cuda as gc
