@@ -68,3 +68,48 @@ def test_dataflow_width_knob():
     finally:
         lib.ggp_set_dataflow_width(old)
     assert lib.ggp_get_dataflow_width() == old == 4.0
+
+
+def _header_params():
+    """{name: (return kind, [parameter kinds])} from the header's declarations, comments removed. Kinds: 'P'
+    (any pointer, the stream handle included), 'I' (int / int32_t / enum), 'I64', 'U64' (uint64_t, size_t),
+    'D' (double), 'V' (void)."""
+    text = re.sub(r"/\*.*?\*/", " ", HEADER.read_text(), flags=re.S)
+    decls = re.findall(r"^\s*((?:const\s+)?\w+\s*\*?)\s+(ggp_\w+)\s*\(([^;{]*?)\)\s*;", text, re.M | re.S)
+
+    def kind(decl):
+        decl = " ".join(decl.split())
+        if "*" in decl or decl.startswith("ggp_stream_t"):
+            return "P"
+        base = decl.replace("const ", "").split()[0]
+        return {"int": "I", "int32_t": "I", "int64_t": "I64", "uint64_t": "U64", "size_t": "U64", "double": "D",
+                "void": "V", "float": "F"}[base]
+
+    out = {}
+    for ret, name, params in decls:
+        ps = [p for p in (s.strip() for s in params.split(",")) if p and p != "void"]
+        out[name] = (kind(ret), [kind(p) for p in ps])
+    return out
+
+
+def _ctypes_kind(t):
+    if t is None:
+        return "V"
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or hasattr(t, "_type_") and isinstance(t._type_, type):
+        return "P"
+    return {ctypes.c_int: "I", ctypes.c_int64: "I64", ctypes.c_uint64: "U64", ctypes.c_size_t: "U64",
+            ctypes.c_double: "D", ctypes.c_float: "F"}[t]
+
+
+def test_ctypes_signatures_match_header():
+    """Every ctypes signature in graphgp_b200/_lib.py has the header's parameter count and kinds, in order (an
+    argument added on one side only would otherwise shift every later argument)."""
+    from graphgp_b200 import _lib
+
+    hdr = _header_params()
+    assert set(hdr) == set(declared_symbols())
+    for name, (args, res) in _lib._SIGS.items():
+        h_ret, h_args = hdr[name]
+        got = [_ctypes_kind(a) for a in args]
+        assert got == h_args, (name, got, h_args)
+        assert _ctypes_kind(res) == h_ret, (name, res, h_ret)
