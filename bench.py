@@ -344,8 +344,8 @@ def run_ours(args, world, rank, local):
 
     extra = {"generate_grad": {"value": n * world / (grad_ms * 1e-3), "unit": "points/s", "ms_per_step": grad_ms,
                                "step": "loss = 0.5|generate(xi) - y|^2 + generate_logdet, loss.backward() through "
-                                       "graphgp_b200.generate_and_logdet (forward values, logdet and per-row "
-                                       "residuals w, a, sigma; one adjoint sweep w.r.t. xi and the table values)",
+                                       "graphgp_b200.generate_and_logdet (forward values and logdet, one adjoint "
+                                       "sweep w.r.t. xi and the table values)",
                                "status_error": gst["error"] if gst else None}}
     # inverse and log-determinant of the same workload (no dependency waits)
     for name, fn in (("inverse", lambda: gc.generate_inv(gp, gi, gn, OF, B, V, out)),
@@ -546,8 +546,7 @@ def differentiation(dev, n_dirs=64, steps=5, warmup=3, n=4194304):
                         "r = 0 + 1,000 log bins on [1e-5, 1.5], jitter 1e-4; loss 0.5|generate(xi) - y|^2 + logdet",
             "value": n / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
             "step": "FP32 loss = 0.5|generate(xi) - y|^2 + logdet and loss.backward() (graphgp_b200.generate_and_logdet: "
-                    "forward values, logdet and per-row residuals, one adjoint sweep; grad w.r.t. 4,194,304 xi and "
-                    "1,001 table values)",
+                    "forward values and logdet, one adjoint sweep; grad w.r.t. 4,194,304 xi and 1,001 table values)",
             "status_error": st["error"] if st else None, "fallback_points": st["fallback_count"] if st else None,
             "fd_directions": n_dirs, "fd_step": h,
             "fd_rel_err_fp32_adjoint": {k: stats(v[0]) for k, v in res.items()},

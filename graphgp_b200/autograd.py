@@ -11,8 +11,8 @@ reverse sweep on the device:
   backward returns d<g, values>/dxi (N,) and d<g, values>/dcov_vals (n_bins,).
 * ``GenerateLogdetFn``: logdet = generate_logdet(cov_vals) (FP64 0-d tensor); its backward returns
   g * dlogdet/dcov_vals through the same adjoint with a zero value cotangent.
-* ``GenerateAndLogdetFn``: both at once, with one adjoint sweep for both cotangents (a Gaussian likelihood). In
-  FP32 with 10 < k <= 20 and d in {2, 3} its forward also keeps each refined row's w, a and sigma (``RESIDUALS``),
+* ``GenerateAndLogdetFn``: both at once, with one adjoint sweep for both cotangents (a Gaussian likelihood). With
+  ``RESIDUALS = True`` (FP32, 10 < k <= 20, d in {2, 3}) its forward also keeps each refined row's w, a and sigma,
   which the backward sweep reads instead of refactorising the row.
 
 The graph (points, neighbours, offsets, indices) and the table's bins are constants: no gradient flows to them.
@@ -24,9 +24,10 @@ import torch
 
 from . import graphgp_cuda as _gc
 
-# GenerateAndLogdetFn keeps each refined row's w, a and sigma from its forward pass ((2k + 1) FP32 per row) so that
-# the backward sweep does not refactorise; False trades that memory for recomputation.
-RESIDUALS = True
+# False (the default): the backward sweep recomputes every refined row's factorisation and nothing per row is kept.
+# True: GenerateAndLogdetFn keeps each refined row's w, a and sigma from its forward pass ((2k + 1) FP32 per row, no
+# Cholesky factor) and the backward sweep reads them instead of refactorising (FP32, 10 < k <= 20, d in {2, 3}).
+RESIDUALS = False
 
 
 class GenerateFn(torch.autograd.Function):
